@@ -1,1 +1,21 @@
-"""B200-native gapped-k-mer SVM kernel path (package body filled in below)."""
+"""B200-native (sm_100a) implementation of gkmsvm-lite's pairwise gapped-k-mer
+kernel path: GkmSVM scoring, score_variants, ISM, GkmExplain and the training
+Gram matrix, with the reference's signatures, computed by hand-written CUDA
+kernels behind the C ABI of include/gkm_b200.h."""
+
+from .explain import gkmexplain, mutation_impact
+from .gram import compute_gram
+from .importers import load_lsgkm_model, load_model
+from .inputs import as_batch, encode_codes, to_codes
+from .ism import ism
+from .kernels import (KERNEL_ALIASES, KERNEL_BUILDERS, CenterWeightedGkmKernel, CenterWeightedRbfGkmKernel,
+                      DirectGkmKernel, EstTruncGkmKernel, GkmKernel, RbfGkmKernel, RbfKernel,
+                      resolve_kernel_type)
+from .model import GkmSVM
+
+__all__ = [
+    "GkmSVM", "ism", "gkmexplain", "mutation_impact", "compute_gram", "load_lsgkm_model", "load_model",
+    "KERNEL_ALIASES", "KERNEL_BUILDERS", "resolve_kernel_type", "GkmKernel", "DirectGkmKernel",
+    "EstTruncGkmKernel", "CenterWeightedGkmKernel", "RbfKernel", "RbfGkmKernel",
+    "CenterWeightedRbfGkmKernel", "as_batch", "encode_codes", "to_codes",
+]

@@ -1,0 +1,613 @@
+// gkm_index.cu -- the SV l-mer index: built by an LSD radix sort of the packed
+// l-mers of every SV window (forward and RC) into per-SV-tile CSR buckets, and
+// queried by visiting each query window's d-mismatch neighbourhood.
+//
+// Query accumulators are integer pair counts per (SV, mismatch level) in
+// shared memory, one SV tile per thread block; the FP64 epilogue weights them
+// by h(m) and, for scoring, normalises, applies the RBF and reduces over the
+// tile's SVs in a fixed order (deterministic), so no [rows, S] block is written.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gkm_common.cuh"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Device-wide exclusive scan of uint32 (three phases, recursive on block sums)
+// ---------------------------------------------------------------------------
+
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_PER_THREAD = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_PER_THREAD;
+
+__global__ void scan_tiles(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, int64_t n,
+                           uint32_t *__restrict__ tile_sums)
+{
+    __shared__ uint32_t warp_tot[32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_PER_THREAD;
+    uint32_t v[SCAN_PER_THREAD];
+    uint32_t run = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER_THREAD; k++) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        uint32_t t = v[k];
+        v[k] = run;
+        run += t;
+    }
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(GKM_FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warp_tot[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(GKM_FULL, w, o);
+            if (lane >= o) w += y;
+        }
+        warp_tot[lane] = w;
+    }
+    __syncthreads();
+    uint32_t excl = x - run + (warp ? warp_tot[warp - 1] : 0);
+#pragma unroll
+    for (int k = 0; k < SCAN_PER_THREAD; k++)
+        if (base + k < n) out[base + k] = v[k] + excl;
+    if (threadIdx.x == SCAN_THREADS - 1 && tile_sums) tile_sums[blockIdx.x] = excl + run;
+}
+
+__global__ void scan_add(uint32_t *__restrict__ out, int64_t n, const uint32_t *__restrict__ tile_pref)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += tile_pref[i / SCAN_TILE];
+}
+
+int scan_exclusive(const uint32_t *in, uint32_t *out, int64_t n, cudaStream_t st)
+{
+    if (n <= 0) return GKM_OK;
+    int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (tiles == 1) {
+        scan_tiles<<<1, SCAN_THREADS, 0, st>>>(in, out, n, nullptr);
+        GKM_CHECK_LAUNCH("scan");
+        return GKM_OK;
+    }
+    uint32_t *sums = nullptr;
+    if (cudaMallocAsync(&sums, sizeof(uint32_t) * tiles * 2, st) != cudaSuccess)
+        return gkm_fail(GKM_ERR_OOM, "scan scratch");
+    scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, sums);
+    GKM_CHECK_LAUNCH("scan");
+    int s = scan_exclusive(sums, sums + tiles, tiles, st);
+    if (s == GKM_OK) {
+        scan_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, n, sums + tiles);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) s = gkm_cuda_status(e, "scan_add");
+    }
+    cudaFreeAsync(sums, st);
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// LSD radix sort of (key, value) pairs, 8-bit digits, stable
+// ---------------------------------------------------------------------------
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_SUB = 16;                       // sub-tiles of 256 keys per block
+constexpr int RS_CHUNK = RS_THREADS * RS_SUB;    // keys per block
+
+__global__ void radix_hist(const uint32_t *__restrict__ keys, int64_t n, int shift, uint32_t *__restrict__ hist,
+                           int64_t nblocks)
+{
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    int64_t base = (int64_t)blockIdx.x * RS_CHUNK;
+    for (int k = threadIdx.x; k < RS_CHUNK; k += RS_THREADS) {
+        int64_t i = base + k;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter: keys of a block go out in their input order within each digit.
+__global__ void radix_scatter(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
+                              uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, int64_t n, int shift,
+                              const uint32_t *__restrict__ pref, int64_t nblocks)
+{
+    constexpr int NWARP = RS_THREADS / 32;
+    __shared__ uint32_t run[256];
+    __shared__ uint32_t wcnt[NWARP][256];
+    __shared__ uint32_t woff[NWARP][256];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    run[threadIdx.x] = pref[(int64_t)threadIdx.x * nblocks + blockIdx.x];
+    int64_t base = (int64_t)blockIdx.x * RS_CHUNK;
+    for (int sub = 0; sub < RS_SUB; sub++) {
+        for (int w = 0; w < NWARP; w++) wcnt[w][threadIdx.x] = 0;
+        __syncthreads();
+        int64_t i = base + (int64_t)sub * RS_THREADS + threadIdx.x;
+        bool valid = i < n;
+        uint32_t k = valid ? kin[i] : 0, v = valid ? vin[i] : 0;
+        uint32_t d = (k >> shift) & 255u;
+        uint32_t act = __ballot_sync(GKM_FULL, valid);
+        uint32_t rank = 0;
+        if (valid) {
+            uint32_t peers = __match_any_sync(act, d);
+            rank = __popc(peers & ((1u << lane) - 1u));
+            if (rank == 0) wcnt[warp][d] = __popc(peers);
+        }
+        __syncthreads();
+        {  // thread t owns digit t: prefix over warps
+            uint32_t s = 0;
+            for (int w = 0; w < NWARP; w++) {
+                woff[w][threadIdx.x] = s;
+                s += wcnt[w][threadIdx.x];
+            }
+            wcnt[0][threadIdx.x] = s;  // sub-tile total for the digit (read after sync)
+        }
+        __syncthreads();
+        if (valid) {
+            uint32_t pos = run[d] + woff[warp][d] + rank;
+            kout[pos] = k;
+            vout[pos] = v;
+        }
+        __syncthreads();
+        run[threadIdx.x] += wcnt[0][threadIdx.x];
+        __syncthreads();
+    }
+}
+
+int radix_sort(uint32_t *&keys, uint32_t *&vals, uint32_t *&ktmp, uint32_t *&vtmp, int64_t n, int bits,
+               cudaStream_t st)
+{
+    if (n <= 1) return GKM_OK;
+    int64_t nb = (n + RS_CHUNK - 1) / RS_CHUNK;
+    uint32_t *hist = nullptr;
+    if (cudaMallocAsync(&hist, sizeof(uint32_t) * 256 * nb * 2, st) != cudaSuccess)
+        return gkm_fail(GKM_ERR_OOM, "radix sort scratch");
+    int s = GKM_OK;
+    for (int shift = 0; shift < bits && s == GKM_OK; shift += 8) {
+        radix_hist<<<(unsigned)nb, RS_THREADS, 0, st>>>(keys, n, shift, hist, nb);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            s = gkm_cuda_status(e, "radix_hist");
+            break;
+        }
+        s = scan_exclusive(hist, hist + 256 * nb, 256 * nb, st);
+        if (s != GKM_OK) break;
+        radix_scatter<<<(unsigned)nb, RS_THREADS, 0, st>>>(keys, vals, ktmp, vtmp, n, shift, hist + 256 * nb, nb);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            s = gkm_cuda_status(e, "radix_scatter");
+            break;
+        }
+        uint32_t *t = keys;
+        keys = ktmp;
+        ktmp = t;
+        t = vals;
+        vals = vtmp;
+        vtmp = t;
+    }
+    cudaFreeAsync(hist, st);
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Index build
+// ---------------------------------------------------------------------------
+
+__global__ void entry_counts(const int32_t *__restrict__ counts, int64_t S, int nb, uint32_t *__restrict__ out)
+{
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < S) out[s] = (uint32_t)counts[s] * nb;
+}
+
+// Entries in column order: each SV's forward windows, then its RC windows in
+// RC-row order (kernels/lmer_index.py:171-176), so a stable sort keeps every
+// bucket ascending by SV.  key = tile << 2l | l-mer; value = local SV id |
+// window weight << 24.
+__global__ void entry_gen(gkm_spec spec, const uint32_t *__restrict__ fwd, const uint32_t *__restrict__ rc,
+                          const int32_t *__restrict__ counts, const uint32_t *__restrict__ base, int64_t S,
+                          int64_t W, int tile_svs, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals)
+{
+    int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= S * W) return;
+    int64_t s = idx / W;
+    int j = (int)(idx - s * W);
+    int n = counts[s];
+    if (j >= n) return;
+    uint32_t tile = (uint32_t)(s / tile_svs);
+    uint32_t local = (uint32_t)(s - (int64_t)tile * tile_svs);
+    uint32_t hi = tile << (2 * spec.l);
+    uint32_t e0 = base[s];
+    uint32_t wf = spec.weighted ? gkm_wt(spec.wd, n, j) : 1u;
+    keys[e0 + j] = hi | fwd[s * W + j];
+    vals[e0 + j] = local | (wf << 24);
+    if (spec.include_rc && rc) {
+        // RC-row position W - n + j holds rc(forward window n - 1 - j)
+        uint32_t wr = spec.weighted ? gkm_wt(spec.wd, n, n - 1 - j) : 1u;
+        keys[e0 + n + j] = hi | rc[s * W + (W - n + j)];
+        vals[e0 + n + j] = local | (wr << 24);
+    }
+}
+
+__global__ void bucket_offsets(const uint32_t *__restrict__ keys, int64_t E, int64_t nbuckets,
+                               uint32_t *__restrict__ off)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > E) return;
+    int64_t lo = i == 0 ? 0 : (int64_t)keys[i - 1] + 1;
+    int64_t hi = i == E ? nbuckets : (int64_t)keys[i];
+    for (int64_t k = lo; k <= hi; k++) off[k] = (uint32_t)i;
+}
+
+// ---------------------------------------------------------------------------
+// Index query
+// ---------------------------------------------------------------------------
+
+constexpr int Q_THREADS = 1024;
+enum { MODE_SCORE = 0, MODE_RAW = 1 };
+
+struct QueryArgs {
+    const uint32_t *bx;
+    const int32_t *cx;
+    int64_t W;
+    const int32_t *order;
+    int64_t diag_offset;  // >= 0: row r is column diag_offset + r
+    // index
+    const uint32_t *off;
+    const uint32_t *ent;
+    const uint32_t *masks;
+    int n_masks;
+    int64_t n_lmers;
+    int64_t S;
+    int tile_svs;
+    int nlev;
+    int dmax;
+    double h[16];
+    const uint8_t *wd;
+    // score
+    const double *inv_dx;
+    const double *inv_ds;
+    const double *coef;
+    double gamma;
+    int rbf;
+    double *partial;  // [B, tiles]
+    // raw
+    double *raw;
+    uint64_t *profile;
+    int l;
+};
+
+template <bool WEIGHTED, int MODE>
+__global__ void __launch_bounds__(Q_THREADS) index_query(QueryArgs a)
+{
+    extern __shared__ uint32_t acc[];  // [nlev][tile_svs]
+    __shared__ double red[32];
+    const int64_t r = blockIdx.x;
+    const int64_t row = a.order ? a.order[r] : r;
+    const int t = blockIdx.y;
+    const int St = a.tile_svs;
+    const int64_t s0 = (int64_t)t * St;
+    const int ns = (int)min((int64_t)St, a.S - s0);
+    int64_t lo_g = a.diag_offset >= 0 ? a.diag_offset + row : 0;
+    if (MODE == MODE_RAW && s0 + ns <= lo_g) return;  // tile wholly below the diagonal
+    const uint32_t lo = (uint32_t)(lo_g > s0 ? lo_g - s0 : 0);
+    const int nacc = a.nlev * St;
+    for (int k = threadIdx.x; k < nacc; k += Q_THREADS) acc[k] = 0;
+    __syncthreads();
+    const int n = a.cx[row];
+    const uint32_t *x = a.bx + row * a.W;
+    const uint32_t *off = a.off + (int64_t)t * a.n_lmers;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = warp; i < n; i += Q_THREADS / 32) {
+        const uint32_t u = x[i];
+        const uint32_t wq = WEIGHTED ? gkm_wt(a.wd, n, i) : 1u;
+        for (int c = lane; c < a.n_masks; c += 32) {
+            const uint32_t mk = __ldg(a.masks + c);
+            const uint32_t v = u ^ (mk & 0x00FFFFFFu);
+            uint32_t *lev = acc + (mk >> 24) * St;
+            const uint32_t beg = __ldg(off + v), end = __ldg(off + v + 1);
+            for (uint32_t e = end; e > beg; e--) {
+                const uint32_t en = __ldg(a.ent + e - 1);
+                const uint32_t id = en & 0x00FFFFFFu;
+                if (id < lo) break;  // bucket ids ascend
+                atomicAdd(lev + id, WEIGHTED ? wq * (en >> 24) : 1u);
+            }
+        }
+    }
+    __syncthreads();
+    double part = 0.0;
+    for (int s = threadIdx.x; s < ns; s += Q_THREADS) {
+        double k = 0.0;
+        for (int m = 0; m < a.nlev; m++) k += a.h[m] * (double)acc[m * St + s];
+        const int64_t sg = s0 + s;
+        if (MODE == MODE_SCORE) {
+            double kn = k * a.inv_dx[row] * a.inv_ds[sg];
+            part += a.coef[sg] * (a.rbf ? exp(a.gamma * (kn - 1.0)) : kn);
+        } else if (s >= (int)lo) {
+            if (a.raw) a.raw[row * a.S + sg] = k;
+            if (a.profile) {
+                uint64_t *p = a.profile + (row * a.S + sg) * (a.l + 1);
+                for (int m = 0; m <= a.l; m++) p[m] = m < a.nlev ? acc[m * St + s] : 0;
+            }
+        }
+    }
+    if (MODE == MODE_SCORE) {
+        part = gkm_block_sum(part, red);
+        if (threadIdx.x == 0) a.partial[row * gridDim.y + t] = part;
+    }
+}
+
+__global__ void finish_scores(const double *__restrict__ partial, int64_t B, int tiles, double bias,
+                              double *__restrict__ out)
+{
+    int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    double s = 0.0;
+    for (int t = 0; t < tiles; t++) s += partial[b * tiles + t];
+    out[b] = s + bias;
+}
+
+// V[v] over every tile's bucket of v (lmer_table.py:35-55)
+__global__ void lmer_weights_kernel(const uint32_t *__restrict__ off, const uint32_t *__restrict__ ent,
+                                    int64_t n_lmers, int tiles, int tile_svs, int weighted,
+                                    const double *__restrict__ c_sv, double *__restrict__ V)
+{
+    int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n_lmers) return;
+    double acc = 0.0;
+    for (int t = 0; t < tiles; t++) {
+        uint32_t b = off[t * n_lmers + v], e = off[t * n_lmers + v + 1];
+        for (uint32_t k = b; k < e; k++) {
+            uint32_t en = ent[k];
+            double c = c_sv[(int64_t)t * tile_svs + (en & 0x00FFFFFFu)];
+            acc += weighted ? c * (double)(en >> 24) : c;
+        }
+    }
+    V[v] = acc;
+}
+
+}  // namespace
+
+int gkm_smem_limit()
+{
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v;
+}
+
+int gkm_sm_count()
+{
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v;
+}
+
+extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const uint32_t *rc,
+                                const int32_t *counts, int64_t S, int64_t W, const uint32_t *masks,
+                                int32_t n_masks, int32_t tile_svs, gkm_index_t **out, gkm_stream_t stream)
+{
+    if (!spec || !out) return gkm_fail(GKM_ERR_INVALID, "null spec or out");
+    *out = nullptr;
+    if (spec->l < 1 || spec->l > 12) return gkm_fail(GKM_ERR_UNSUPPORTED, "the l-mer index needs l <= 12");
+    if (S < 1 || W < 1) return gkm_fail(GKM_ERR_INVALID, "empty columns");
+    if (S > (1 << 24) * 64LL) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many columns");
+    if (!masks || n_masks < 1) return gkm_fail(GKM_ERR_INVALID, "no neighbour masks");
+    if (spec->weighted && !spec->wd) return gkm_fail(GKM_ERR_INVALID, "weighted spec without weights");
+    cudaStream_t st = (cudaStream_t)stream;
+    int nlev = spec->dmax + 1;
+    int smem = gkm_smem_limit() - 1024;
+    int max_tile = smem / (4 * nlev);
+    if (tile_svs <= 0) {
+        int64_t T = (S + max_tile - 1) / max_tile;
+        tile_svs = (int32_t)((S + T - 1) / T);
+    }
+    if (tile_svs > max_tile || tile_svs > (1 << 24)) return gkm_fail(GKM_ERR_INVALID, "tile_svs %d too large", tile_svs);
+    int64_t T = (S + tile_svs - 1) / tile_svs;
+    int tile_bits = 0;
+    while ((1LL << tile_bits) < T) tile_bits++;
+    if (2 * spec->l + tile_bits > 32) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many SV tiles for l = %d", spec->l);
+    int nb = (spec->include_rc && rc) ? 2 : 1;
+
+    gkm_index *ix = new gkm_index();
+    ix->spec = *spec;
+    ix->S = S;
+    ix->W = W;
+    ix->tiles = (int32_t)T;
+    ix->tile_svs = tile_svs;
+    ix->nlev = nlev;
+    ix->n_lmers = (int64_t)1 << (2 * spec->l);
+    ix->n_masks = n_masks;
+    int status = GKM_OK;
+    uint32_t *ecount = nullptr, *base = nullptr, *keys = nullptr, *vals = nullptr, *kt = nullptr, *vt = nullptr;
+    uint32_t total = 0;
+    int64_t nbuckets = T * ix->n_lmers;
+    do {
+        if (cudaMallocAsync(&ecount, sizeof(uint32_t) * (S + 1) * 2, st) != cudaSuccess) {
+            status = gkm_fail(GKM_ERR_OOM, "index build scratch");
+            break;
+        }
+        base = ecount + S + 1;
+        entry_counts<<<(unsigned)((S + 255) / 256), 256, 0, st>>>(counts, S, nb, ecount);
+        cudaMemsetAsync(ecount + S, 0, sizeof(uint32_t), st);
+        if ((status = scan_exclusive(ecount, base, S + 1, st)) != GKM_OK) break;
+        if (cudaMemcpyAsync(&total, base + S, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            status = gkm_cuda_status(cudaGetLastError(), "index size");
+            break;
+        }
+        ix->entries = total;
+        size_t eb = sizeof(uint32_t) * (total ? total : 1);
+        if (cudaMallocAsync(&keys, eb, st) != cudaSuccess || cudaMallocAsync(&vals, eb, st) != cudaSuccess ||
+            cudaMallocAsync(&kt, eb, st) != cudaSuccess || cudaMallocAsync(&vt, eb, st) != cudaSuccess) {
+            status = gkm_fail(GKM_ERR_OOM, "index entries (%u)", total);
+            break;
+        }
+        int64_t n = S * W;
+        entry_gen<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(*spec, fwd, rc, counts, base, S, W, tile_svs, keys, vals);
+        GKM_CHECK_LAUNCH("entry_gen");
+        if ((status = radix_sort(keys, vals, kt, vt, total, 2 * spec->l + tile_bits, st)) != GKM_OK) break;
+        if (cudaMalloc(&ix->offsets, sizeof(uint32_t) * (nbuckets + 1)) != cudaSuccess) {
+            status = gkm_fail(GKM_ERR_OOM, "index offsets");
+            break;
+        }
+        bucket_offsets<<<(unsigned)((total + 1 + 255) / 256), 256, 0, st>>>(keys, total, nbuckets, ix->offsets);
+        GKM_CHECK_LAUNCH("bucket_offsets");
+        if (cudaMalloc(&ix->ent, eb) != cudaSuccess || cudaMalloc(&ix->masks, sizeof(uint32_t) * n_masks) != cudaSuccess) {
+            status = gkm_fail(GKM_ERR_OOM, "index entries");
+            break;
+        }
+        cudaMemcpyAsync(ix->ent, vals, eb, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(ix->masks, masks, sizeof(uint32_t) * n_masks, cudaMemcpyDeviceToDevice, st);
+        ix->bytes = (int64_t)sizeof(uint32_t) * (nbuckets + 1) + (int64_t)eb + sizeof(uint32_t) * n_masks;
+    } while (0);
+    cudaFreeAsync(ecount, st);
+    cudaFreeAsync(keys, st);
+    cudaFreeAsync(vals, st);
+    cudaFreeAsync(kt, st);
+    cudaFreeAsync(vt, st);
+    if (status == GKM_OK) {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) status = gkm_cuda_status(e, "index build");
+    }
+    if (status != GKM_OK) {
+        gkm_index_free(ix);
+        return status;
+    }
+    *out = ix;
+    return GKM_OK;
+}
+
+extern "C" int gkm_index_free(gkm_index_t *ix)
+{
+    if (!ix) return GKM_OK;
+    cudaFree(ix->offsets);
+    cudaFree(ix->ent);
+    cudaFree(ix->masks);
+    delete ix;
+    return GKM_OK;
+}
+
+extern "C" int gkm_index_info(const gkm_index_t *ix, int64_t *entries, int32_t *tiles, int32_t *tile_svs,
+                              int64_t *device_bytes)
+{
+    if (!ix) return gkm_fail(GKM_ERR_INVALID, "null index");
+    if (entries) *entries = ix->entries;
+    if (tiles) *tiles = ix->tiles;
+    if (tile_svs) *tile_svs = ix->tile_svs;
+    if (device_bytes) *device_bytes = ix->bytes;
+    return GKM_OK;
+}
+
+static QueryArgs query_args(const gkm_index_t *ix, const uint32_t *bx, const int32_t *cx, int64_t W)
+{
+    QueryArgs a = {};
+    a.bx = bx;
+    a.cx = cx;
+    a.W = W;
+    a.diag_offset = -1;
+    a.off = ix->offsets;
+    a.ent = ix->ent;
+    a.masks = ix->masks;
+    a.n_masks = ix->n_masks;
+    a.n_lmers = ix->n_lmers;
+    a.S = ix->S;
+    a.tile_svs = ix->tile_svs;
+    a.nlev = ix->nlev;
+    a.dmax = ix->spec.dmax;
+    for (int m = 0; m < 16; m++) a.h[m] = ix->spec.h[m];
+    a.wd = ix->spec.wd;
+    a.l = ix->spec.l;
+    return a;
+}
+
+template <int MODE>
+static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cudaStream_t st)
+{
+    size_t smem = sizeof(uint32_t) * (size_t)ix->nlev * ix->tile_svs;
+    dim3 grid((unsigned)B, (unsigned)ix->tiles);
+    if (ix->spec.weighted) {
+        cudaFuncSetAttribute(index_query<true, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        index_query<true, MODE><<<grid, Q_THREADS, smem, st>>>(a);
+    } else {
+        cudaFuncSetAttribute(index_query<false, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        index_query<false, MODE><<<grid, Q_THREADS, smem, st>>>(a);
+    }
+    GKM_CHECK_LAUNCH("index_query");
+    return GKM_OK;
+}
+
+extern "C" int gkm_index_pairwise(const gkm_index_t *ix, const uint32_t *bx, const int32_t *cx, int64_t B,
+                                  int64_t W, int64_t diag_offset, double *raw, uint64_t *profile,
+                                  gkm_stream_t stream)
+{
+    if (!ix || !bx || !cx) return gkm_fail(GKM_ERR_INVALID, "null index or rows");
+    if (B == 0) return GKM_OK;
+    QueryArgs a = query_args(ix, bx, cx, W);
+    a.diag_offset = diag_offset;
+    a.raw = raw;
+    a.profile = profile;
+    return query_launch<MODE_RAW>(ix, a, B, (cudaStream_t)stream);
+}
+
+extern "C" int gkm_index_score(const gkm_index_t *ix, const uint32_t *bx, const int32_t *cx, int64_t B,
+                               int64_t W, const double *inv_dx, const double *inv_ds, const double *coef,
+                               double gamma, int32_t rbf, double bias, const int32_t *order, double *scores,
+                               gkm_stream_t stream)
+{
+    if (!ix || !bx || !cx || !inv_dx || !inv_ds || !coef || !scores)
+        return gkm_fail(GKM_ERR_INVALID, "null argument");
+    if (B == 0) return GKM_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    double *partial = nullptr;
+    if (cudaMallocAsync(&partial, sizeof(double) * B * ix->tiles, st) != cudaSuccess)
+        return gkm_fail(GKM_ERR_OOM, "score partials");
+    QueryArgs a = query_args(ix, bx, cx, W);
+    a.order = order;
+    a.inv_dx = inv_dx;
+    a.inv_ds = inv_ds;
+    a.coef = coef;
+    a.gamma = gamma;
+    a.rbf = rbf;
+    a.partial = partial;
+    int s = query_launch<MODE_SCORE>(ix, a, B, st);
+    if (s == GKM_OK) {
+        finish_scores<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(partial, B, ix->tiles, bias, scores);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) s = gkm_cuda_status(e, "finish_scores");
+    }
+    cudaFreeAsync(partial, st);
+    return s;
+}
+
+extern "C" int gkm_index_lmer_weights(const gkm_index_t *ix, const double *c_sv, double *V, gkm_stream_t stream)
+{
+    if (!ix || !c_sv || !V) return gkm_fail(GKM_ERR_INVALID, "null argument");
+    int64_t n = ix->n_lmers;
+    lmer_weights_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        ix->offsets, ix->ent, n, ix->tiles, ix->tile_svs, ix->spec.weighted, c_sv, V);
+    GKM_CHECK_LAUNCH("lmer_weights");
+    return GKM_OK;
+}
+
+extern "C" int gkm_index_mutants(const gkm_index_t *, const uint32_t *, const int32_t *, int64_t, int64_t, int64_t,
+                                 const double *, const double *, const double *, const double *, const double *,
+                                 const double *, double, int32_t, double *, gkm_stream_t)
+{
+    return gkm_fail(GKM_ERR_UNSUPPORTED, "gkm_index_mutants: not built yet");
+}
+
+extern "C" int gkm_explain_lmer(const gkm_spec *, const uint32_t *, const int32_t *, int64_t, int64_t, int64_t,
+                                const double *, const double *, const gkm_index_t *, const double *,
+                                const uint32_t *, int32_t, const double *, const double *, int32_t, double *,
+                                gkm_stream_t)
+{
+    return gkm_fail(GKM_ERR_UNSUPPORTED, "gkm_explain_lmer: not built yet");
+}

@@ -1,0 +1,198 @@
+"""Device operations on torch tensors: thin wrappers over the C ABI.
+
+Every function takes and returns CUDA tensors and enqueues its work on the
+current torch stream; nothing here synchronises except index creation (which
+reads the entry count back) and explicit capacity checks.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr
+
+U32 = torch.int32  # uint32 words are stored in int32 tensors (bit patterns)
+
+
+def _st():
+    return _lib.stream_handle()
+
+
+class Spec:
+    """gkm_spec of a base kernel, with its window-weight table on the device."""
+
+    def __init__(self, base, device: torch.device):
+        self.base = base
+        self.device = device
+        s = _lib.GkmSpec()
+        s.l = base.l
+        s.include_rc = int(bool(base.include_rc))
+        s.weighted = int(bool(base.weighted))
+        s.dmax = base.dmax
+        h = np.zeros(16)
+        h[: base.l + 1] = base._mismatch_table
+        for m in range(16):
+            s.h[m] = float(h[m])
+        self.wd = None
+        if base.weighted:
+            self.wd = torch.from_numpy(base._wd).to(device)
+            s.wd = self.wd.data_ptr()
+            s.wd_len = int(self.wd.numel())
+        self.c = s
+        self.ref = ctypes.byref(s)
+
+    def check_rows(self, counts_max: int):
+        if self.wd is not None and counts_max >= self.c.wd_len:
+            raise ValueError(f"rows of {counts_max} windows exceed the weight table")
+
+
+def pack(spec: Spec, codes: torch.Tensor, lengths) -> tuple:
+    """(fwd [B, W], rc [B, W] or None, counts [B] int32)."""
+    B, L = codes.shape
+    l = spec.base.l
+    if L < l:
+        raise ValueError(f"Sequence length {L} is shorter than window length {l}")
+    W = L - l + 1
+    dev = codes.device
+    fwd = torch.empty((B, W), dtype=U32, device=dev)
+    rc = torch.empty((B, W), dtype=U32, device=dev) if spec.base.include_rc else None
+    counts = torch.empty(B, dtype=torch.int32, device=dev)
+    ln = None
+    if lengths is not None:
+        ln = torch.as_tensor(np.asarray(lengths, dtype=np.int64)).to(dev, non_blocking=True)
+    call("gkm_pack", spec.ref, ptr(codes), ptr(ln), B, L, ptr(fwd), ptr(rc), ptr(counts), _st())
+    return fwd, rc, counts
+
+
+def self_kernel(spec: Spec, fwd, rc, counts, profile: bool = False):
+    B, W = fwd.shape
+    diag = torch.empty(B, dtype=torch.float64, device=fwd.device)
+    prof = torch.empty((B, spec.base.l + 1), dtype=torch.int64, device=fwd.device) if profile else None
+    call("gkm_self_kernel", spec.ref, ptr(fwd), ptr(rc), ptr(counts), B, W, ptr(diag), ptr(prof), _st())
+    return (diag, prof) if profile else diag
+
+
+def join_pairwise(spec: Spec, bx, cx, by, ry, cy, raw: bool = True, profile: bool = False):
+    B, Wx = bx.shape
+    S, Wy = by.shape
+    out = torch.empty((B, S), dtype=torch.float64, device=bx.device) if raw else None
+    prof = torch.empty((B, S, spec.base.l + 1), dtype=torch.int64, device=bx.device) if profile else None
+    call("gkm_join_pairwise", spec.ref, ptr(bx), ptr(cx), B, Wx, ptr(by), ptr(ry), ptr(cy), S, Wy,
+         ptr(out), ptr(prof), _st())
+    return out, prof
+
+
+def masks_tensor(base, device) -> torch.Tensor:
+    m = base.masks()
+    return torch.from_numpy(m.view(np.int32).copy()).to(device)
+
+
+class DeviceIndex:
+    """An l-mer index handle over packed columns (owned; freed on close)."""
+
+    def __init__(self, spec: Spec, fwd, rc, counts, masks: torch.Tensor, tile_svs: int = 0):
+        self.spec = spec
+        self.S = fwd.shape[0]
+        self.masks = masks
+        h = ctypes.c_void_p()
+        call("gkm_index_create", spec.ref, ptr(fwd), ptr(rc), ptr(counts), fwd.shape[0], fwd.shape[1],
+             ptr(masks), int(masks.numel()), int(tile_svs), ctypes.byref(h), _st())
+        self.handle = h
+        e, t, ts, nb = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        call("gkm_index_info", h, ctypes.byref(e), ctypes.byref(t), ctypes.byref(ts), ctypes.byref(nb))
+        self.entries, self.tiles, self.tile_svs, self.nbytes = e.value, t.value, ts.value, nb.value
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            _lib.load().gkm_index_free(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def pairwise(self, bx, cx, diag_offset=None, raw=True, profile=False, out=None):
+        B, W = bx.shape
+        if raw and out is None:
+            out = torch.zeros((B, self.S), dtype=torch.float64, device=bx.device)
+        prof = (torch.zeros((B, self.S, self.spec.base.l + 1), dtype=torch.int64, device=bx.device)
+                if profile else None)
+        call("gkm_index_pairwise", self.handle, ptr(bx), ptr(cx), B, W,
+             -1 if diag_offset is None else int(diag_offset), ptr(out if raw else None), ptr(prof), _st())
+        return out, prof
+
+    def score(self, bx, cx, inv_dx, inv_ds, coef, gamma, rbf, bias, order=None, out=None):
+        B, W = bx.shape
+        if out is None:
+            out = torch.empty(B, dtype=torch.float64, device=bx.device)
+        call("gkm_index_score", self.handle, ptr(bx), ptr(cx), B, W, ptr(inv_dx), ptr(inv_ds), ptr(coef),
+             float(gamma), int(rbf), float(bias), ptr(order), ptr(out), _st())
+        return out
+
+    def lmer_weights(self, c_sv):
+        n = 4**self.spec.base.l
+        V = torch.empty(n, dtype=torch.float64, device=c_sv.device)
+        call("gkm_index_lmer_weights", self.handle, ptr(c_sv), ptr(V), _st())
+        return V
+
+
+def lmer_table(spec: Spec, V, masks):
+    table = torch.empty_like(V)
+    call("gkm_lmer_table", spec.ref, ptr(V), ptr(masks), int(masks.numel()), ptr(table), _st())
+    return table
+
+
+def table_score(spec: Spec, table, fwd, rc, counts, bias, normalize, want_parts=False):
+    B, W = fwd.shape
+    dev = fwd.device
+    scores = torch.empty(B, dtype=torch.float64, device=dev)
+    raw = torch.empty(B, dtype=torch.float64, device=dev) if want_parts else None
+    diag = torch.empty(B, dtype=torch.float64, device=dev) if want_parts else None
+    call("gkm_table_score", spec.ref, ptr(table), ptr(fwd), ptr(rc), ptr(counts), B, W, float(bias),
+         int(bool(normalize)), ptr(scores), ptr(raw), ptr(diag), _st())
+    return (scores, raw, diag) if want_parts else scores
+
+
+def raw_score(raw, dx, ds, coef, gamma, rbf, bias):
+    B, S = raw.shape
+    out = torch.empty(B, dtype=torch.float64, device=raw.device)
+    call("gkm_raw_score", ptr(raw), B, S, ptr(dx), ptr(ds), ptr(coef), float(gamma), int(rbf), float(bias),
+         ptr(out), _st())
+    return out
+
+
+def impact(raw, n, dr, ds, coef, gamma, rbf):
+    S = raw.shape[1]
+    out = torch.empty(n, dtype=torch.float64, device=raw.device)
+    call("gkm_impact", ptr(raw), n, S, ptr(dr), ptr(ds), ptr(coef), float(gamma), int(rbf), ptr(out), _st())
+    return out
+
+
+def mutant_diag(spec: Spec, fwd, counts, L, diag):
+    B, W = fwd.shape
+    out = torch.empty((4, L, B), dtype=torch.float64, device=fwd.device)
+    call("gkm_mutant_diag", spec.ref, ptr(fwd), ptr(counts), B, W, L, ptr(diag), ptr(out), _st())
+    return out
+
+
+def ism_table(spec: Spec, table, fwd, counts, L, ref_raw, diag, normalize, want_mut=False):
+    B, W = fwd.shape
+    out = torch.empty((B, 4, L), dtype=torch.float64, device=fwd.device)
+    mut = torch.empty((4, L, B), dtype=torch.float64, device=fwd.device) if want_mut else None
+    call("gkm_ism_table", spec.ref, ptr(table), ptr(fwd), ptr(counts), B, W, L, ptr(ref_raw),
+         ptr(diag if normalize else None), ptr(mut), int(bool(normalize)), ptr(out), _st())
+    return (out, mut) if want_mut else out
+
+
+def gram_finish(raw, dx, dy, gamma, rbf, symmetric):
+    N, M = raw.shape
+    out = torch.empty_like(raw)
+    call("gkm_gram_finish", ptr(raw), N, M, ptr(dx), ptr(dy), float(gamma), int(rbf), int(symmetric),
+         ptr(out), _st())
+    return out

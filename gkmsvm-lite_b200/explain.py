@@ -1,0 +1,180 @@
+"""GkmExplain attributions and the GkmExplain mutation impact on the GPU
+(explain/core.py:34-247, explain/lmer.py, explain/impact.py of gkmsvm-lite).
+
+Attributions go through l-mer weights: each query window visits the l-mers
+within the explain cutoff and adds alpha/kappa (or the perturbation deltas)
+times the neighbour's weight to each of its positions.  The weight of a
+neighbour v is V[v] = sum_s coef_s / sqrt(K(sv, sv)) (occurrences of v in sv_s
+and its RC) for linear kernels, and for RBF kernels the per-query SV weights
+summed over the l-mer index's entries of v (gkm_explain_lmer).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import engine
+from ._lib import call, ptr, stream_handle
+from .inputs import (allele_arrays, as_batch, device_codes, joint_lengths, nan_rows, per_position, rows,
+                     short_rows)
+from .kernels import RbfKernel, explain_tables, neighbor_masks
+
+_MODE_ALIASES = {0: "importance", 1: "hypothetical", 2: "perturbation", "importance": "importance",
+                 "hypothetical": "hypothetical", "perturbation": "perturbation"}
+
+
+def _rbf_scale(k_norm: torch.Tensor, gamma: float) -> torch.Tensor:
+    pos = k_norm > 0
+    safe = torch.where(pos, k_norm, torch.ones_like(k_norm))
+    return torch.where(pos, (torch.exp(gamma * (safe - 1)) - np.exp(-gamma)) / safe, torch.zeros_like(k_norm))
+
+
+def _explain_masks(model, perturbation: bool, dev):
+    base = model.kernel.base
+    a, b, dmax = explain_tables(base, perturbation)
+    key = ("explain_masks", perturbation)
+    c = model._sv_cache
+    if key not in c:
+        nonzero = tuple(bool(a[m] != 0 or b[m] != 0) for m in range(base.l + 1))
+        masks = neighbor_masks(base.l, nonzero, dmax)
+        c[key] = (torch.from_numpy(masks.view(np.int32).copy()).to(dev),
+                  torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev))
+    return c[key]
+
+
+def _explain_V(model) -> torch.Tensor:
+    """V[v] = sum_s coef_s / sqrt(K(sv, sv)) over the window-weighted
+    occurrences of l-mer v in each SV and its RC (explain/common.py:87-98)."""
+    c = model._sv_cache
+    if "explain_V" not in c:
+        spec = model._spec()
+        fwd, rc, counts = model._sv_packed()
+        coef = model._sv_coef() * model._inv_ds()
+        index = c.get("index")
+        tmp = None
+        if index is None:
+            tmp = engine.DeviceIndex(spec, fwd, rc, counts, model._masks())
+            index = tmp
+        c["explain_V"] = index.lmer_weights(coef.contiguous())
+        if tmp is not None:
+            tmp.close()
+    return c["explain_V"]
+
+
+def gkmexplain(model, x, *, mode="importance", lengths=None, batch_size=50, verbose=False) -> torch.Tensor:
+    """[B, 4, L] float64 attributions (explain/core.py:34-113): importance =
+    hypothetical x one-hot (N credited to A), hypothetical, or perturbation."""
+    resolved = _MODE_ALIASES.get(mode)
+    if resolved is None:
+        raise ValueError(f"mode must be 'importance', 'hypothetical', or 'perturbation' (or 0/1/2), got {mode!r}")
+    dev = model._require_gpu()
+    x, lengths = as_batch(x, lengths)
+    short = short_rows(lengths, model.kernel.base.l, "attributions")
+    B, L = x.shape
+    bs = max(1, int(batch_size)) if batch_size else B
+    parts = []
+    it = range(0, B, bs)
+    if verbose:
+        from tqdm import tqdm
+        it = tqdm(it, desc="GkmExplain")
+    for s in it:
+        parts.append(_explain_rows(model, x[s:s + bs], rows(lengths, s, bs), resolved, dev))
+    out = parts[0] if len(parts) == 1 else torch.cat(parts)
+    return per_position(out, lengths, short)
+
+
+def _explain_rows(model, x, lengths, mode, dev):
+    kernel = model.kernel
+    base = kernel.base
+    spec = model._spec()
+    L = x.shape[-1]
+    if L < base.l:
+        return torch.full((x.shape[0], 4, L), float("nan"), dtype=torch.float64, device=dev)
+    xt = device_codes(x, dev)
+    fwd, rc, counts = engine.pack(spec, xt, lengths)
+    spec.check_rows(int(fwd.shape[1]))
+    perturbation = mode == "perturbation"
+    masks, ta, tb = _explain_masks(model, perturbation, dev)
+    B, W = fwd.shape
+    if base.normalize:
+        dx = engine.self_kernel(spec, fwd, rc, counts)
+        inv_dx = 1.0 / torch.sqrt(torch.clamp(dx, min=1e-20))
+    else:
+        inv_dx = torch.ones(B, dtype=torch.float64, device=dev)
+    V = index = w = None
+    if isinstance(kernel, RbfKernel):
+        index = model._sv_index()
+        if index is None:
+            raise NotImplementedError("RBF GkmExplain needs the l-mer index")
+        raw, _ = index.pairwise(fwd, counts)
+        inv_ds = model._inv_ds()
+        k_norm = raw * inv_dx[:, None] * inv_ds[None, :]
+        w = (model._sv_coef() * inv_ds)[None, :] * _rbf_scale(k_norm, kernel.gamma)
+        w = w.contiguous()
+    else:
+        V = _explain_V(model)
+    out = torch.empty((B, 4, L), dtype=torch.float64, device=dev)
+    call("gkm_explain_lmer", spec.ref, ptr(fwd), ptr(counts), B, W, L, ptr(inv_dx), ptr(V),
+         None if index is None else index.handle, ptr(w), ptr(masks), int(masks.numel()), ptr(ta), ptr(tb),
+         int(perturbation), ptr(out), stream_handle())
+    if mode == "importance":
+        oh = torch.nn.functional.one_hot(xt.long(), 4).permute(0, 2, 1).to(out.dtype)
+        out = out * oh
+    return out
+
+
+def mutation_impact(model, ref, alt, *, ref_lengths=None, alt_lengths=None, batch_size=None,
+                    verbose=False) -> torch.Tensor:
+    """[B, 1] GkmExplain mutation impact (lsgkm gkmexplain -m 5,
+    explain/impact.py:51-194): sum_j coef_j dK_j with K normalised by the
+    reference allele's norm; RBF kernels scale each SV by
+    (exp(g (K_j - 1)) - exp(-g)) / K_j."""
+    dev = model._require_gpu()
+    kernel = model.kernel
+    base = kernel.base
+    ref, alt, ref_lengths, alt_lengths = allele_arrays(ref, alt, ref_lengths, alt_lengths)
+    L = ref.shape[-1]
+    B = ref.shape[0]
+    short = None
+    if ref_lengths is not None or alt_lengths is not None:
+        both_l = joint_lengths(L, (B, ref_lengths), (B, alt_lengths))
+        s = short_rows(both_l, base.l, "mutation impacts")
+        if s is not None:
+            short = s.reshape(2, -1).any(axis=0)
+    W = max(L - base.l + 1, 0)
+    model._plan_lmer_table(B * 2 * (min(base.l, W) if model._index_applies() else W))
+    if L < base.l:
+        return torch.full((B, 1), float("nan"), dtype=torch.float64, device=dev)
+    spec = model._spec()
+    bs = B if batch_size is None else max(1, batch_size)
+    parts = []
+    rbf = isinstance(kernel, RbfKernel)
+    gamma = kernel.gamma if rbf else 0.0
+    for s in range(0, B, bs):
+        r, a = ref[s:s + bs], alt[s:s + bs]
+        n = r.shape[0]
+        both = torch.cat([device_codes(r, dev), device_codes(a, dev)])
+        bl = joint_lengths(L, (n, rows(ref_lengths, s, bs)), (n, rows(alt_lengths, s, bs)))
+        fwd, rc, counts = engine.pack(spec, both, bl)
+        spec.check_rows(int(fwd.shape[1]))
+        table = model._lmer_table_for()
+        if table is not None:
+            _, raw, diag = engine.table_score(spec, table, fwd, rc, counts, 0.0, base.normalize,
+                                              want_parts=True)
+            dk = raw[n:] - raw[:n]
+            if base.normalize:
+                dk = dk / torch.sqrt(torch.clamp(diag[:n], min=1e-10))
+            parts.append(dk)
+            continue
+        dr = engine.self_kernel(spec, fwd[:n], None if rc is None else rc[:n], counts[:n]) if base.normalize else None
+        index = model._sv_index()
+        if index is not None:
+            kb, _ = index.pairwise(fwd, counts)
+        else:
+            by, ry, cy = model._sv_packed()
+            kb, _ = engine.join_pairwise(spec, fwd, counts, by, ry, cy)
+        ds = model._sv_diag() if base.normalize else None
+        parts.append(engine.impact(kb, n, dr, ds, model._sv_coef(), gamma, rbf))
+    out = torch.cat(parts)[:, None]
+    return nan_rows(out, short)

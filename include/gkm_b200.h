@@ -1,0 +1,196 @@
+/*
+ * gkm_b200.h -- C ABI of the B200 (sm_100a) gapped-k-mer kernel library.
+ *
+ * Plain pointers and sizes; every array argument is DEVICE memory unless its
+ * comment says host; every call is asynchronous on the given CUDA stream and
+ * returns a status (GKM_OK = 0).  gkm_last_error() describes the last failure
+ * of the calling thread.
+ *
+ * Each entry point replaces one operation of gkmsvm-lite's kernel operator
+ * API (paths relative to its source tree, src/gkmsvm/); that operator is cited
+ * beside it.  Packed windows: a window of l bases is a uint32 with position k
+ * in bits 2k..2k+1 (A=0 C=1 G=2 T=3); GKM_PAD marks no window (past a shorter
+ * row's last window; first in a reverse-complement row).
+ */
+#ifndef GKM_B200_H
+#define GKM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *gkm_stream_t; /* cudaStream_t */
+
+#define GKM_PAD 0xFFFFFFFFu
+#define GKM_MAX_L 15
+
+enum {
+    GKM_OK = 0,
+    GKM_ERR_INVALID = 1,     /* bad argument: shape, l, null pointer ...      */
+    GKM_ERR_CUDA = 2,        /* a CUDA call failed                            */
+    GKM_ERR_OOM = 3,         /* device memory exhausted                        */
+    GKM_ERR_CAPACITY = 4,    /* a counter or table limit was exceeded          */
+    GKM_ERR_UNSUPPORTED = 5  /* the shape needs a path this build lacks        */
+};
+
+/* A kernel type after KERNEL_BUILDERS (svm.py:95-106): the pair weight h(m)
+ * by mismatch count and the window weights of -t 4/-t 5. */
+typedef struct gkm_spec {
+    int32_t l;          /* window length, 1..15 */
+    int32_t include_rc; /* 1: the reverse complement adds a column block */
+    int32_t weighted;   /* 1: centre-weighted windows (kernels/weighted.py) */
+    int32_t dmax;       /* largest m with h[m] != 0 */
+    double h[16];       /* h[m], m = 0..l; 0 past dmax */
+    const uint8_t *wd;  /* device [wd_len]: window weight by |n/2 - i| */
+    int32_t wd_len;     /* > the longest row's window count when weighted */
+} gkm_spec;
+
+typedef struct gkm_index gkm_index_t; /* SV l-mer index (opaque) */
+
+int gkm_version(void);
+const char *gkm_last_error(void);
+/* Number of SMs of the current device and its opt-in shared memory per block. */
+int gkm_device_info(int32_t *sm_count, int32_t *smem_per_block);
+
+/* Packed forward and RC windows of [B, L] base codes; counts[b] = windows of
+ * row b, lengths (nullable) = each row's length.
+ * Replaces PackedGkmKernel.pack / pack_both (kernels/packed.py:130-187). */
+int gkm_pack(const gkm_spec *spec, const uint8_t *codes, const int64_t *lengths,
+             int64_t B, int64_t L, uint32_t *fwd, uint32_t *rc, int32_t *counts,
+             gkm_stream_t stream);
+
+/* K_raw(x, x) [B] (and, nullable, its profile [B, l+1] of pair counts by
+ * mismatch count, forward and RC blocks summed).
+ * Replaces raw_diag_packed (kernels/direct.py:109-137, 294-306;
+ * kernels/weighted.py:91-118, 440-471). */
+int gkm_self_kernel(const gkm_spec *spec, const uint32_t *fwd, const uint32_t *rc,
+                    const int32_t *counts, int64_t B, int64_t W, double *diag,
+                    uint64_t *profile, gkm_stream_t stream);
+
+/* Pairwise K_raw [B, S] (nullable) and profiles [B, S, l+1] (nullable) of rows
+ * bx against columns by (+ their RC ry when include_rc) by warp ballot/popc
+ * over every window pair.
+ * Replaces PackedGkmKernel.raw_packed's pair loop (kernels/packed.py:191-228,
+ * kernels/direct.py:23-42, kernels/weighted.py:47-69). */
+int gkm_join_pairwise(const gkm_spec *spec, const uint32_t *bx, const int32_t *cx,
+                      int64_t B, int64_t Wx, const uint32_t *by, const uint32_t *ry,
+                      const int32_t *cy, int64_t S, int64_t Wy, double *raw,
+                      uint64_t *profile, gkm_stream_t stream);
+
+/* Builds the l-mer index over S columns (radix sort of the packed l-mers of
+ * their forward and RC windows into per-SV-tile CSR buckets).  masks [n_masks]
+ * (device): the XOR neighbour masks within dmax, each with its mismatch count
+ * in bits 24..31.  tile_svs 0: chosen for shared memory.
+ * Replaces LmerIndex.__init__ (kernels/lmer_index.py:161-200). */
+int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const uint32_t *rc,
+                     const int32_t *counts, int64_t S, int64_t W, const uint32_t *masks,
+                     int32_t n_masks, int32_t tile_svs, gkm_index_t **out,
+                     gkm_stream_t stream);
+int gkm_index_free(gkm_index_t *index);
+int gkm_index_info(const gkm_index_t *index, int64_t *entries, int32_t *tiles,
+                   int32_t *tile_svs, int64_t *device_bytes);
+
+/* K_raw [B, S] (nullable) and profiles [B, S, l+1] (nullable) through the
+ * index; diag_offset >= 0: row b is column diag_offset + b of a self-Gram and
+ * only its columns from there on are written.
+ * Replaces LmerIndex.pairwise (kernels/lmer_index.py:239-268, 400-441). */
+int gkm_index_pairwise(const gkm_index_t *index, const uint32_t *bx, const int32_t *cx,
+                       int64_t B, int64_t W, int64_t diag_offset, double *raw,
+                       uint64_t *profile, gkm_stream_t stream);
+
+/* scores[b] = sum_s coef[s] f(K_raw(b, s) inv_dx[b] inv_ds[s]) + bias, f the
+ * identity or exp(gamma (k - 1)) (rbf), with no [B, S] block.  order
+ * (nullable, [B]): the order rows are handed out in.
+ * Replaces LmerIndex.reduce (kernels/lmer_index.py:275-298,
+ * kernels/lmer_index_cpu.py:71-120) and GkmSVM._sv_scores (svm.py:368-405). */
+int gkm_index_score(const gkm_index_t *index, const uint32_t *bx, const int32_t *cx,
+                    int64_t B, int64_t W, const double *inv_dx, const double *inv_ds,
+                    const double *coef, double gamma, int32_t rbf, double bias,
+                    const int32_t *order, double *scores, gkm_stream_t stream);
+
+/* V[v] = sum over index entries of l-mer v of c_sv[sv] times the entry's
+ * window weight, [4^l].
+ * Replaces sv_lmer_weights (lmer_table.py:35-55). */
+int gkm_index_lmer_weights(const gkm_index_t *index, const double *c_sv, double *V,
+                           gkm_stream_t stream);
+
+/* table[u] = sum_{v within dmax of u} h(m(u, v)) V[v] over all 4^l l-mers.
+ * Replaces build_lmer_table (lmer_table.py:58-98). */
+int gkm_lmer_table(const gkm_spec *spec, const double *V, const uint32_t *masks,
+                   int32_t n_masks, double *table, gkm_stream_t stream);
+
+/* scores[b] = sum_i wt_i table[x_i] / sqrt(max(K(x, x), 1e-10)) + bias (plain
+ * sum without normalize); raw and diag (nullable) get the two parts.
+ * Replaces GkmSVM._table_raw / _score_lmer_table (svm.py:559-582). */
+int gkm_table_score(const gkm_spec *spec, const double *table, const uint32_t *fwd,
+                    const uint32_t *rc, const int32_t *counts, int64_t B, int64_t W,
+                    double bias, int32_t normalize, double *scores, double *raw,
+                    double *diag, gkm_stream_t stream);
+
+/* K_raw(mutant, mutant) [4, L, B] for every single-base substitution, from the
+ * pairs touching the windows that cover the substituted base.
+ * Replaces raw_diag_mutants (kernels/direct.py:160-201, 265-292;
+ * kernels/weighted.py:153-197). */
+int gkm_mutant_diag(const gkm_spec *spec, const uint32_t *fwd, const int32_t *counts,
+                    int64_t B, int64_t W, int64_t L, const double *diag,
+                    double *mut_diag, gkm_stream_t stream);
+
+/* ISM deltas [B, 4, L] from the l-mer table; with normalize the mutant
+ * self-kernels are computed in the same pass (written to mut_diag [4, L, B]
+ * when it is not null) and diag = K(x, x) is required; 0 past each row's
+ * windows.  ref_raw [B] = sum_i wt_i table[x_i].
+ * Replaces _ism_table (ism.py:118-144) with _mutants (ism.py:254-273). */
+int gkm_ism_table(const gkm_spec *spec, const double *table, const uint32_t *fwd,
+                  const int32_t *counts, int64_t B, int64_t W, int64_t L,
+                  const double *ref_raw, const double *diag, double *mut_diag,
+                  int32_t normalize, double *out, gkm_stream_t stream);
+
+/* ISM deltas [B, 4, L] through the index for any kernel (RBF included):
+ * K(mutant, s) = ref_raw[b, s] + K(new windows, s) - K(old windows, s).
+ * Replaces LmerIndex.mutants (kernels/lmer_index.py:326-374,
+ * kernels/lmer_index_cpu.py:203-285). */
+int gkm_index_mutants(const gkm_index_t *index, const uint32_t *fwd, const int32_t *counts,
+                      int64_t B, int64_t W, int64_t L, const double *ref_raw,
+                      const double *ref_score, const double *inv_dx,
+                      const double *mut_diag, const double *inv_ds, const double *coef,
+                      double gamma, int32_t rbf, double *out, gkm_stream_t stream);
+
+/* scores[b] = sum_s coef[s] f(raw[b, s] / max(sqrt(dx[b] ds[s]), 1e-10)) + bias
+ * over a materialised [B, S] block (dx, ds nullable: no normalisation).
+ * Replaces _normalized_dot (svm.py:42-61). */
+int gkm_raw_score(const double *raw, int64_t B, int64_t S, const double *dx,
+                  const double *ds, const double *coef, double gamma, int32_t rbf,
+                  double bias, double *scores, gkm_stream_t stream);
+
+/* Mutation impact [n] from raw [2n, S] = [ref rows; alt rows].
+ * Replaces _impact_cpu (explain/impact.py:22-48). */
+int gkm_impact(const double *raw, int64_t n, int64_t S, const double *dr,
+               const double *ds, const double *coef, double gamma, int32_t rbf,
+               double *out, gkm_stream_t stream);
+
+/* GkmExplain through l-mer weights: each query window visits the l-mers within
+ * the explain cutoff (masks with their mismatch count in bits 24..31) and adds
+ * a(m) or b(m) times the neighbour's weight to each position.  Weights come
+ * from V [4^l] (non-RBF) or, with index and w [B, S], from the sum of w[b, sv]
+ * over the index entries of the neighbour (RBF).  out [B, 4, L].
+ * Replaces _explain_lmer_cpu / _explain_index_cpu (explain/cpu.py:69-207). */
+int gkm_explain_lmer(const gkm_spec *spec, const uint32_t *fwd, const int32_t *counts,
+                     int64_t B, int64_t W, int64_t L, const double *inv_dx,
+                     const double *V, const gkm_index_t *index, const double *w,
+                     const uint32_t *masks, int32_t n_masks, const double *table_a,
+                     const double *table_b, int32_t perturbation, double *out,
+                     gkm_stream_t stream);
+
+/* Normalised, finished Gram [N, M] from raw (upper triangle when symmetric,
+ * mirrored exactly).  Replaces compute_gram's tile finish (gram.py:82-106). */
+int gkm_gram_finish(const double *raw, int64_t N, int64_t M, const double *dx,
+                    const double *dy, double gamma, int32_t rbf, int32_t symmetric,
+                    double *out, gkm_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GKM_B200_H */

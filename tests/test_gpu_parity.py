@@ -1,0 +1,235 @@
+"""GPU parity: the CUDA path against the oracle (bit-exact mismatch profiles)
+and against gkmsvm-lite's own outputs (tests/golden) within the reference's
+GPU tolerance, rtol 1e-9 / atol 1e-12 (its tests/test_gpu.py:100-104).
+Every call goes through the C ABI (libgkm_b200.so)."""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN, LSGKM, codes_of, read_fasta, read_pred
+from oracle import oracle as orc
+
+import gkmsvm_lite_b200 as gk
+from gkmsvm_lite_b200 import engine
+
+pytestmark = pytest.mark.gpu
+RTOL, ATOL = 1e-9, 1e-12
+CASES = ["t2", "t2norc", "t0", "t0small", "t1", "t3", "t4", "t5", "t6"]
+LINEAR = ["t2", "t2norc", "t0", "t0small", "t1", "t4"]
+
+
+def _np(t):
+    return t.detach().cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+
+
+def _model(c, **switches):
+    m = gk.GkmSVM(c["sv"], c["coef"], float(c["bias"]), c["kernel_type"], c["params"],
+                  sv_lengths=c["sv_lengths"]).cuda()
+    for k, v in switches.items():
+        setattr(m, k, v)
+    return m
+
+
+def _okd(c):
+    return orc.KernelDef.from_params(c["kernel_type"], c["params"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_pack_matches_oracle(small, name):
+    c = small[name]
+    m = _model(c)
+    x, xl = c["x"], c["x_lengths"]
+    fwd, rc, counts = engine.pack(m._spec(), torch.from_numpy(x).cuda(), xl)
+    of, orr = orc.pack(x, xl, m.kernel.l)
+    np.testing.assert_array_equal(_np(fwd).view(np.uint32), of)
+    if rc is not None:
+        np.testing.assert_array_equal(_np(rc).view(np.uint32), orr)
+    np.testing.assert_array_equal(_np(counts), np.clip(xl - m.kernel.l + 1, 0, x.shape[1] - m.kernel.l + 1))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_self_profiles_bit_exact(small, name):
+    c = small[name]
+    m = _model(c)
+    kd = _okd(c)
+    fwd, rc, counts = m._sv_packed()
+    diag, prof = engine.self_kernel(m._spec(), fwd, rc, counts, profile=True)
+    want = orc.self_profiles(c["sv"], c["sv_lengths"], kd)
+    d = kd.dmax
+    np.testing.assert_array_equal(_np(prof)[:, : d + 1].astype(np.uint64), want[:, : d + 1])
+    np.testing.assert_allclose(_np(diag), c["diag_sv"], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("path", ["join", "index"])
+def test_pairwise_profiles_bit_exact(small, name, path):
+    c = small[name]
+    m = _model(c)
+    kd = _okd(c)
+    spec = m._spec()
+    bx, _, cx = engine.pack(spec, torch.from_numpy(c["x"]).cuda(), c["x_lengths"])
+    by, ry, cy = m._sv_packed()
+    if path == "join":
+        raw, prof = engine.join_pairwise(spec, bx, cx, by, ry, cy, profile=True)
+    else:
+        if not m.kernel.base.index_applies():
+            pytest.skip("neighbourhood too large for the index")
+        ix = engine.DeviceIndex(spec, by, ry, cy, m._masks(), tile_svs=5)  # several tiles
+        raw, prof = ix.pairwise(bx, cx, profile=True)
+        ix.close()
+    want = orc.profiles(c["x"], c["x_lengths"], c["sv"], c["sv_lengths"], kd)
+    d = kd.dmax
+    np.testing.assert_array_equal(_np(prof)[..., : d + 1].astype(np.uint64), want[..., : d + 1])
+    np.testing.assert_allclose(_np(raw), c["raw"], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("switch", ["auto", "index", "join", "table"])
+def test_scores_match_reference(small, name, switch):
+    c = small[name]
+    sw = {"index": dict(use_lmer_table=False), "join": dict(use_lmer_table=False, use_lmer_index=False),
+          "table": dict(use_lmer_table=True), "auto": {}}[switch]
+    m = _model(c, **sw)
+    with pytest.warns(UserWarning):
+        got = m(c["x"], lengths=c["x_lengths"])
+    np.testing.assert_allclose(_np(got), c["scores"], rtol=RTOL, atol=ATOL)
+    assert np.isnan(_np(got)[-1, 0])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_variant_scores_match_reference(small, name):
+    c = small[name]
+    m = _model(c)
+    ref, rl, alt, al = c["x"][:-1], c["x_lengths"][:-1], c["alt"], c["alt_lengths"]
+    got = m.score_variants(ref, alt, ref_lengths=rl, alt_lengths=al)
+    np.testing.assert_allclose(_np(got), c["variant_kernel"], rtol=RTOL, atol=ATOL)
+    got = m.score_variants(ref, alt, method="gkmexplain", ref_lengths=rl, alt_lengths=al)
+    np.testing.assert_allclose(_np(got), c["variant_impact"], rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.parametrize("name", LINEAR)
+@pytest.mark.parametrize("table", [True, False])
+def test_ism_linear_matches_reference(small, name, table):
+    c = small[name]
+    m = _model(c, use_lmer_table=table)
+    if not table and not m._index_applies():
+        pytest.skip("no index for this kernel")
+    with pytest.warns(UserWarning):
+        got = gk.ism(m, c["x"], lengths=c["x_lengths"])
+    np.testing.assert_allclose(_np(got), c["ism"], rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gram_matches_reference(small, name):
+    c = small[name]
+    m = _model(c)
+    got = gk.compute_gram(m.kernel, c["sv"], lengths=c["sv_lengths"])
+    np.testing.assert_allclose(got, c["gram"], rtol=RTOL, atol=ATOL)
+    assert (got == got.T).all()
+
+
+def test_mutant_diag_matches_oracle(small):
+    """K(mutant, mutant) from the window-delta kernel equals the self-kernel of
+    each mutant sequence."""
+    c = small["t4"]
+    m = _model(c)
+    kd = _okd(c)
+    x, xl = c["x"][:2], c["x_lengths"][:2]
+    spec = m._spec()
+    fwd, rc, counts = engine.pack(spec, torch.from_numpy(x).cuda(), xl)
+    diag = engine.self_kernel(spec, fwd, rc, counts)
+    L = x.shape[1]
+    mut = _np(engine.mutant_diag(spec, fwd, counts, L, diag))
+    for b in range(2):
+        n = int(xl[b])
+        mutants = np.repeat(x[b:b + 1, :n], 4 * n, axis=0)
+        for p in range(n):
+            for v in range(4):
+                mutants[4 * p + v, p] = v
+        want = orc.raw_from_profiles(orc.self_profiles(mutants, None, kd), kd).reshape(n, 4).T
+        np.testing.assert_allclose(mut[:, :n, b], want, rtol=1e-12, atol=1e-12)
+
+
+def test_config1_scores_match_reference():
+    """Plain scoring workload: 2,000 SVs x 300 bp, 1,000 queries (t=2), every path."""
+    import gkmsvm_lite_b200.synthetic as syn
+
+    w = syn.config1()
+    want = np.load(os.path.join(GOLDEN, "config1.npz"))["scores"]
+    for sw in ({"use_lmer_table": False}, {"use_lmer_table": True}, {}):
+        m = gk.GkmSVM(w.sv, w.coef, 0.0, "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}).cuda()
+        for k, v in sw.items():
+            setattr(m, k, v)
+        np.testing.assert_allclose(_np(m(w.x)), want, rtol=RTOL, atol=ATOL)
+
+
+def test_config3_subsample_matches_reference():
+    """72,000-SV model (SV lengths 200..500), queries 50..2000 bp with N: t=2
+    (256 queries) and t=3 gamma=2 (48 queries) against the reference."""
+    import gkmsvm_lite_b200.synthetic as syn
+
+    sv, svl, coef = syn.config3_model()
+    xq, xl, _ = syn.config3_queries()
+    z = np.load(os.path.join(GOLDEN, "config3.npz"))
+    for name, kt, p, n in (("t2", "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, 256),
+                           ("t3", "gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 2.0}, 48)):
+        m = gk.GkmSVM(sv, coef, 0.0, kt, p, sv_lengths=svl).cuda()
+        m.use_lmer_table = False
+        L = int(xl[:n].max())
+        got = _np(m(xq[:n, :L], lengths=xl[:n]))
+        np.testing.assert_allclose(got, z[f"{name}/scores"], rtol=RTOL, atol=ATOL)
+        if name == "t2":
+            np.testing.assert_allclose(_np(m._sv_diag())[:256], z["t2/diag_sv_head"], rtol=1e-12)
+            m.use_lmer_table = True
+            np.testing.assert_allclose(_np(m(xq[:n, :L], lengths=xl[:n])), z["t2/scores"], rtol=RTOL, atol=ATOL)
+
+
+def test_config4_ism_matches_reference():
+    import gkmsvm_lite_b200.synthetic as syn
+
+    sv, svl, coef = syn.config3_model()
+    x = syn.config4_queries()[:2]
+    z = np.load(os.path.join(GOLDEN, "config4.npz"))
+    m = gk.GkmSVM(sv, coef, 0.0, "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, sv_lengths=svl).cuda()
+    m.use_lmer_table = True
+    got = _np(gk.ism(m, x))
+    np.testing.assert_allclose(got, z["ism"], rtol=RTOL, atol=1e-10 * np.abs(z["ism"]).max())
+
+
+def test_config2_gram_matches_reference():
+    import gkmsvm_lite_b200.synthetic as syn
+
+    X, lengths = syn.config2()
+    z = np.load(os.path.join(GOLDEN, "config2.npz"))
+    k = gk.CenterWeightedGkmKernel(11, 7, d=3)
+    rows = gk.compute_gram(k, X[:48], X, lengths=lengths[:48], y_lengths=lengths)
+    np.testing.assert_allclose(rows, z["rows"], rtol=RTOL, atol=ATOL)
+    sym = gk.compute_gram(k, X[:160], lengths=lengths[:160])
+    np.testing.assert_allclose(sym, z["sym"], rtol=RTOL, atol=ATOL)
+
+
+_WGKM = ["t0", "t1", "t2", "t2w2", "t3", "t4", "t4w05", "t5", "t6"]
+
+
+@pytest.mark.parametrize("t", _WGKM)
+def test_lsgkm_gkmpredict(t):
+    m = gk.load_lsgkm_model(os.path.join(LSGKM, f"lsgkm_wgkm_{t}.model.txt.gz")).cuda()
+    for n in (85, 100):
+        _, seqs = read_fasta(os.path.join(LSGKM, f"lsgkm_wgkm_test{n}.fa"))
+        want = read_pred(os.path.join(LSGKM, f"lsgkm_wgkm_{t}_test{n}.pred.txt"))
+        np.testing.assert_allclose(_np(m(seqs))[:, 0], want, rtol=2e-5, atol=1e-5)
+
+
+def test_encode_10sv_gkmpredict():
+    m = gk.load_lsgkm_model(os.path.join(LSGKM, "encode_ENCFF579AOX_10sv.model.txt.gz")).cuda()
+    rows = [line.rstrip("\n").split("\t") for line in open(os.path.join(LSGKM, "encode_10sv_gkmpredict.tsv"))]
+    for i, (name, seq, want) in enumerate(rows):
+        if name.startswith("sv"):
+            n = m.sv_lengths[i] if m.sv_lengths is not None else m.support_sequences.shape[1]
+            x = m.support_sequences[i:i + 1, :n]
+        else:
+            x = [seq]
+        assert abs(float(_np(m(x))[0, 0]) - float(want)) < 1e-4

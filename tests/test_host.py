@@ -1,0 +1,139 @@
+"""Host-side logic without a GPU: kernel tables, neighbour masks and window
+weights against the oracle; input handling; the C ABI library exports every
+symbol include/gkm_b200.h declares."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from oracle import oracle as orc
+
+import gkmsvm_lite_b200 as gk
+from gkmsvm_lite_b200 import kernels as K
+from gkmsvm_lite_b200 import inputs
+
+PARAMS = [
+    ("gkm_esttrunc", {"L": 11, "k": 7, "d": 3}),
+    ("gkm_estfull", {"L": 8, "k": 5, "d": 2}),
+    ("gkm_cnt", {"L": 7, "k": 4}),
+    ("gkm_cnt", {"L": 10, "k": 6, "d": 3}),
+    ("gkmrbf", {"L": 10, "k": 6, "d": 3, "gamma": 2.0}),
+    ("wgkm", {"L": 9, "k": 6, "d": 2, "M": 20, "H": 10.0}),
+    ("wgkmrbf", {"L": 11, "k": 7, "d": 3}),
+    ("gkm_cnt_rbf", {"L": 8, "k": 5, "d": 2, "gamma": 1.5}),
+    ("gkm_esttrunc", {"L": 15, "k": 8, "d": 4}),
+]
+
+
+@pytest.mark.parametrize("kt,p", PARAMS)
+def test_tables_equal_oracle(kt, p):
+    kd = orc.KernelDef.from_params(kt, p)
+    k = K.KERNEL_BUILDERS[K.resolve_kernel_type(kt)](p)
+    np.testing.assert_array_equal(k.base._mismatch_table, kd.h)
+    assert k.base.dmax == kd.dmax
+    assert isinstance(k, K.RbfKernel) == kd.rbf
+
+
+@pytest.mark.parametrize("kt,p", PARAMS[:8])
+def test_neighbor_masks_equal_oracle(kt, p):
+    kd = orc.KernelDef.from_params(kt, p)
+    base = K.KERNEL_BUILDERS[K.resolve_kernel_type(kt)](p).base
+    masks = base.masks()
+    om, ol = orc.neighbor_masks(kd.l, kd.h, kd.dmax)
+    np.testing.assert_array_equal(masks & 0x00FFFFFF, om)
+    np.testing.assert_array_equal(masks >> 24, ol)
+
+
+def test_mask_count_l11_d3():
+    base = K.EstTruncGkmKernel(11, 7, d=3)
+    assert len(base.masks()) == 4984 == K.neighbor_count(11, 3)
+    assert base.index_applies() and base.has_table()
+
+
+@pytest.mark.parametrize("M,H", [(50, 50.0), (20, 10.0), (255, 3.5), (1, 1.0)])
+def test_window_weights_bit_identical(M, H):
+    k = K.CenterWeightedGkmKernel(10, 6, M=M, H=H)
+    for W in (1, 2, 7, 90, 91, 290, 1990):
+        np.testing.assert_array_equal(k.window_weights(W), orc.window_weights(W, M, H))
+
+
+def test_resolve_kernel_type():
+    assert K.resolve_kernel_type(2) == "gkm_esttrunc"
+    assert K.resolve_kernel_type("5") == "wgkmrbf"
+    assert K.resolve_kernel_type("direct_rbf") == "gkm_cnt_rbf"
+    with pytest.raises(ValueError):
+        K.resolve_kernel_type(9)
+    with pytest.raises(NotImplementedError):
+        K.resolve_kernel_type("nope")
+
+
+def test_kernel_argument_checks():
+    with pytest.raises(ValueError):
+        K.DirectGkmKernel(16, 4)
+    with pytest.raises(ValueError):
+        K.EstTruncGkmKernel(5, 7)
+    with pytest.raises(ValueError):
+        K.CenterWeightedGkmKernel(10, 6, M=0)
+
+
+def test_as_batch_strings_and_one_hot():
+    x, ln = inputs.as_batch(["ACGTN", "GG"])
+    np.testing.assert_array_equal(x, [[0, 1, 2, 3, 0], [2, 2, 0, 0, 0]])
+    np.testing.assert_array_equal(ln, [5, 2])
+    oh = np.eye(4)[[[0, 1, 2, 3]]].transpose(0, 2, 1)
+    oh[0, :, 1] = 0  # N reads as A
+    np.testing.assert_array_equal(inputs.to_codes(oh), [[0, 0, 2, 3]])
+    with pytest.raises(ValueError):
+        inputs.as_batch(np.zeros((2, 5), np.uint8), lengths=[1, 9])
+    assert inputs.as_batch(np.zeros((2, 5), np.uint8), lengths=[5, 5])[1] is None
+
+
+def test_allele_arrays_pad_indels():
+    ref, alt, rl, al = inputs.allele_arrays(["ACGTA"], ["ACGTAAC"])
+    assert ref.shape == alt.shape == (1, 7)
+    np.testing.assert_array_equal(rl, [5])
+    assert al is None
+
+
+def test_model_on_cpu_refuses_to_compute():
+    m = gk.GkmSVM(np.zeros((3, 20), np.uint8), np.ones(3), 0.0, 2, {"L": 11, "k": 7, "d": 3})
+    with pytest.raises(RuntimeError, match="CUDA only"):
+        m(np.zeros((1, 20), np.uint8))
+
+
+def test_lsgkm_loader_matches_oracle():
+    from conftest import LSGKM
+
+    p = os.path.join(LSGKM, "lsgkm_ragged_t4.model.txt.gz")
+    m = gk.load_lsgkm_model(p)
+    om = orc.load_lsgkm(p)
+    np.testing.assert_array_equal(m.support_sequences, om.sv)
+    np.testing.assert_array_equal(m.sv_lengths, om.sv_lengths)
+    np.testing.assert_array_equal(m.coefficients, om.coef)
+    assert m.bias == om.bias and m.kernel_type == "wgkm"
+
+
+def _declared_symbols():
+    src = open(os.path.join(ROOT, "include", "gkm_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gkm_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_abi_library_exports_every_declared_symbol():
+    from gkmsvm_lite_b200 import _lib
+
+    if not os.path.exists(_lib.LIB_PATH):
+        from gkmsvm_lite_b200 import build
+        build.build()
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    names = _declared_symbols()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) <= set(_lib.SIGNATURES) | {"gkm_last_error"}
+    lib.gkm_version.restype = ctypes.c_int
+    assert lib.gkm_version() >= 1
