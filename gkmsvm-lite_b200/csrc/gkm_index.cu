@@ -270,6 +270,7 @@ struct QueryArgs {
     int dmax;
     double h[16];
     const uint8_t *wd;
+    const uint8_t *wq;    // [rows, W] query window weights (null: from the row's count)
     // score
     const double *inv_dx;
     const double *inv_ds;
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(Q_THREADS) index_query(QueryArgs a)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = warp; i < n; i += Q_THREADS / 32) {
         const uint32_t u = x[i];
-        const uint32_t wq = WEIGHTED ? gkm_wt(a.wd, n, i) : 1u;
+        const uint32_t wq = WEIGHTED ? (a.wq ? (uint32_t)a.wq[row * a.W + i] : gkm_wt(a.wd, n, i)) : 1u;
         for (int c = lane; c < a.n_masks; c += 32) {
             const uint32_t mk = __ldg(a.masks + c);
             const uint32_t v = u ^ (mk & 0x00FFFFFFu);
@@ -597,17 +598,134 @@ extern "C" int gkm_index_lmer_weights(const gkm_index_t *ix, const double *c_sv,
     return GKM_OK;
 }
 
-extern "C" int gkm_index_mutants(const gkm_index_t *, const uint32_t *, const int32_t *, int64_t, int64_t, int64_t,
-                                 const double *, const double *, const double *, const double *, const double *,
-                                 const double *, double, int32_t, double *, gkm_stream_t)
+// ---------------------------------------------------------------------------
+// ISM through the index (kernels/lmer_index_cpu.py:203-285): per (position p,
+// row b), the windows covering p before (set 0) and after each substitution v
+// (sets 1..4) are queried as rows of <= l windows that keep their slot weights
+// (ism.py:276-295); then K(mutant, s) = ref[b, s] + K(set v, s) - K(set 0, s).
+// ---------------------------------------------------------------------------
+
+__global__ void ism_sets_kernel(gkm_spec spec, const uint32_t *__restrict__ fwd, const int32_t *__restrict__ cnt,
+                                int64_t B, int64_t W, int64_t p0, int64_t nitems, uint32_t *__restrict__ rows,
+                                int32_t *__restrict__ rcount, uint8_t *__restrict__ rwt)
 {
-    return gkm_fail(GKM_ERR_UNSUPPORTED, "gkm_index_mutants: not built yet");
+    int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= nitems) return;
+    const int l = spec.l;
+    int64_t p = p0 + it / B, b = it % B;
+    int n = cnt[b];
+    int a_s = (int)(p - l + 1 > 0 ? p - l + 1 : 0);
+    int a_e = (int)(p + 1 < n ? p + 1 : n);
+    int na = a_e > a_s ? a_e - a_s : 0;
+    for (int r = 0; r < 5; r++) {
+        int64_t row = it * 5 + r;
+        rcount[row] = na;
+        for (int j = 0; j < l; j++) {
+            uint32_t w = GKM_PAD;
+            uint8_t wt = 0;
+            if (j < na) {
+                int i = a_s + j;
+                w = fwd[b * W + i];
+                if (r > 0) {
+                    uint32_t sh = 2u * (uint32_t)(p - i);
+                    w = (w & ~(3u << sh)) | ((uint32_t)(r - 1) << sh);
+                }
+                wt = spec.weighted ? (uint8_t)gkm_wt(spec.wd, n, i) : 1;
+            }
+            rows[row * l + j] = w;
+            if (rwt) rwt[row * l + j] = wt;
+        }
+    }
 }
 
-extern "C" int gkm_explain_lmer(const gkm_spec *, const uint32_t *, const int32_t *, int64_t, int64_t, int64_t,
-                                const double *, const double *, const gkm_index_t *, const double *,
-                                const uint32_t *, int32_t, const double *, const double *, int32_t, double *,
-                                gkm_stream_t)
+__global__ void ism_index_finish(const double *__restrict__ kset, int64_t S, const uint32_t *__restrict__ fwd,
+                                 const int32_t *__restrict__ cnt, int64_t B, int64_t W, int64_t L, int l,
+                                 int64_t p0, const double *__restrict__ ref, const double *__restrict__ ref_score,
+                                 const double *__restrict__ inv_dx, const double *__restrict__ inv_dmut,
+                                 const double *__restrict__ inv_ds, const double *__restrict__ coef,
+                                 double gamma, int rbf, double *__restrict__ out)
 {
-    return gkm_fail(GKM_ERR_UNSUPPORTED, "gkm_explain_lmer: not built yet");
+    __shared__ double red[32];
+    int64_t it = blockIdx.x;
+    int64_t p = p0 + it / B, b = it % B;
+    int n = cnt[b];
+    int a_s = (int)(p - l + 1 > 0 ? p - l + 1 : 0);
+    int a_e = (int)(p + 1 < n ? p + 1 : n);
+    // the base at p as packed in the first window covering it
+    int xp = a_e > a_s ? (int)((fwd[b * W + a_s] >> (2 * (p - a_s))) & 3u) : -1;
+    const double *k0 = kset + (it * 5) * S;
+    const double *rr = ref + b * S;
+    for (int v = 0; v < 4; v++) {
+        double z = inv_dmut[((int64_t)v * L + p) * B + b];
+        bool same = a_e <= a_s || (v == xp && z == inv_dx[b]);
+        if (same) {  // the reference's windows and norm: exactly 0
+            if (threadIdx.x == 0) out[(b * 4 + v) * L + p] = 0.0;
+            continue;
+        }
+        const double *kv = kset + (it * 5 + 1 + v) * S;
+        double acc = 0.0;
+        for (int64_t s = threadIdx.x; s < S; s += blockDim.x) {
+            double k = (rr[s] + (kv[s] - k0[s])) * z * inv_ds[s];
+            acc += coef[s] * (rbf ? exp(gamma * (k - 1.0)) : k);
+        }
+        acc = gkm_block_sum(acc, red);
+        if (threadIdx.x == 0) out[(b * 4 + v) * L + p] = acc - ref_score[b];
+    }
 }
+
+extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, const int32_t *counts, int64_t B,
+                                 int64_t W, int64_t L, const double *ref_raw, const double *ref_score,
+                                 const double *inv_dx, const double *inv_dmut, const double *inv_ds,
+                                 const double *coef, double gamma, int32_t rbf, double *out, gkm_stream_t stream)
+{
+    if (!ix || !fwd || !counts || !ref_raw || !ref_score || !inv_dx || !inv_dmut || !inv_ds || !coef || !out)
+        return gkm_fail(GKM_ERR_INVALID, "null argument");
+    if (B == 0 || L == 0) return GKM_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int l = ix->spec.l;
+    const int64_t S = ix->S;
+    int64_t per_item = 5 * S * (int64_t)sizeof(double);
+    int64_t chunk = (1LL << 30) / per_item;
+    if (chunk < 1) chunk = 1;
+    int64_t total = L * B;
+    if (chunk > total) chunk = total;
+    if (chunk > (1LL << 31) - 1) chunk = (1LL << 31) - 1;
+    chunk = (chunk / B) * B;  // whole positions per chunk
+    if (chunk < B) chunk = B;
+    uint32_t *rows = nullptr;
+    int32_t *rc = nullptr;
+    uint8_t *rw = nullptr;
+    double *kset = nullptr;
+    int s = GKM_OK;
+    if (cudaMallocAsync(&rows, sizeof(uint32_t) * chunk * 5 * l, st) != cudaSuccess ||
+        cudaMallocAsync(&rc, sizeof(int32_t) * chunk * 5, st) != cudaSuccess ||
+        cudaMallocAsync(&rw, chunk * 5 * l, st) != cudaSuccess ||
+        cudaMallocAsync(&kset, sizeof(double) * chunk * 5 * S, st) != cudaSuccess)
+        s = gkm_fail(GKM_ERR_OOM, "ISM scratch");
+    for (int64_t p0 = 0; s == GKM_OK && p0 < L; p0 += chunk / B) {
+        int64_t np = chunk / B;
+        if (p0 + np > L) np = L - p0;
+        int64_t nitems = np * B;
+        ism_sets_kernel<<<(unsigned)((nitems + 127) / 128), 128, 0, st>>>(ix->spec, fwd, counts, B, W, p0, nitems,
+                                                                           rows, rc, rw);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            s = gkm_cuda_status(e, "ism_sets");
+            break;
+        }
+        QueryArgs a = query_args(ix, rows, rc, l);
+        a.wq = ix->spec.weighted ? rw : nullptr;
+        a.raw = kset;
+        if ((s = query_launch<MODE_RAW>(ix, a, nitems * 5, st)) != GKM_OK) break;
+        ism_index_finish<<<(unsigned)nitems, 256, 0, st>>>(kset, S, fwd, counts, B, W, L, l, p0, ref_raw, ref_score,
+                                                           inv_dx, inv_dmut, inv_ds, coef, gamma, rbf, out);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) s = gkm_cuda_status(e, "ism_index_finish");
+    }
+    cudaFreeAsync(rows, st);
+    cudaFreeAsync(rc, st);
+    cudaFreeAsync(rw, st);
+    cudaFreeAsync(kset, st);
+    return s;
+}
+

@@ -123,6 +123,29 @@ def test_ism_linear_matches_reference(small, name, table):
 
 
 @pytest.mark.parametrize("name", CASES)
+def test_ism_index_matches_reference(small, name):
+    """ISM through the l-mer index (every kernel type, RBF included)."""
+    c = small[name]
+    m = _model(c, use_lmer_table=False)
+    if not m._index_applies():
+        pytest.skip("no index for this kernel")
+    with pytest.warns(UserWarning):
+        got = gk.ism(m, c["x"], lengths=c["x_lengths"])
+    np.testing.assert_allclose(_np(got), c["ism"], rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("mode,key", [("hypothetical", "explain_hyp"), ("importance", "explain_imp"),
+                                      ("perturbation", "explain_pert")])
+def test_explain_matches_reference(small, name, mode, key):
+    c = small[name]
+    m = _model(c)
+    with pytest.warns(UserWarning):
+        got = gk.gkmexplain(m, c["x"], lengths=c["x_lengths"], mode=mode)
+    np.testing.assert_allclose(_np(got), c[key], rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.parametrize("name", CASES)
 def test_gram_matches_reference(small, name):
     c = small[name]
     m = _model(c)
@@ -199,6 +222,36 @@ def test_config4_ism_matches_reference():
     np.testing.assert_allclose(got, z["ism"], rtol=RTOL, atol=1e-10 * np.abs(z["ism"]).max())
 
 
+def test_config4_explain_matches_reference():
+    import gkmsvm_lite_b200.synthetic as syn
+
+    sv, svl, coef = syn.config3_model()
+    x = syn.config4_queries()[:2]
+    z = np.load(os.path.join(GOLDEN, "config4.npz"))
+    m = gk.GkmSVM(sv, coef, 0.0, "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, sv_lengths=svl).cuda()
+    got = _np(gk.gkmexplain(m, x, mode="hypothetical"))
+    np.testing.assert_allclose(got, z["explain_hyp"], rtol=RTOL, atol=1e-10 * np.abs(z["explain_hyp"]).max())
+
+
+def test_config5_mixed_requests_match_reference():
+    """72,000-SV t=5 (wgkmrbf) model: predict (with a row shorter than l),
+    variant scores with indels, ISM and GkmExplain."""
+    import gkmsvm_lite_b200.synthetic as syn
+
+    sv, svl, coef = syn.config3_model()
+    z = np.load(os.path.join(GOLDEN, "config5.npz"))
+    m = gk.GkmSVM(sv, coef, 0.0, "wgkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 1.0}, sv_lengths=svl).cuda()
+    with pytest.warns(UserWarning):
+        got = _np(m(z["x"], lengths=z["x_lengths"]))
+    np.testing.assert_allclose(got, z["scores"], rtol=RTOL, atol=ATOL)
+    got = _np(m.score_variants(z["ref"], z["alt"], ref_lengths=z["ref_lengths"], alt_lengths=z["alt_lengths"]))
+    np.testing.assert_allclose(got, z["variants"], rtol=RTOL, atol=ATOL)
+    got = _np(gk.ism(m, z["ism_x"]))
+    np.testing.assert_allclose(got, z["ism"], rtol=RTOL, atol=1e-10 * np.abs(z["ism"]).max())
+    got = _np(gk.gkmexplain(m, z["ism_x"], mode="hypothetical"))
+    np.testing.assert_allclose(got, z["explain_hyp"], rtol=RTOL, atol=1e-10 * np.abs(z["explain_hyp"]).max())
+
+
 def test_config2_gram_matches_reference():
     import gkmsvm_lite_b200.synthetic as syn
 
@@ -221,6 +274,34 @@ def test_lsgkm_gkmpredict(t):
         _, seqs = read_fasta(os.path.join(LSGKM, f"lsgkm_wgkm_test{n}.fa"))
         want = read_pred(os.path.join(LSGKM, f"lsgkm_wgkm_{t}_test{n}.pred.txt"))
         np.testing.assert_allclose(_np(m(seqs))[:, 0], want, rtol=2e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("t", ["t0", "t1", "t4", "t5", "t6"])
+@pytest.mark.parametrize("lm,mode", [(0, "importance"), (1, "hypothetical"), (4, "perturbation")])
+def test_lsgkm_gkmexplain(t, lm, mode):
+    from conftest import read_lsgkm_explain
+
+    m = gk.load_lsgkm_model(os.path.join(LSGKM, f"lsgkm_wgkm_{t}.model.txt.gz")).cuda()
+    _, seqs = read_fasta(os.path.join(LSGKM, "lsgkm_wgkm_test85.fa"))
+    want = read_lsgkm_explain(os.path.join(LSGKM, f"lsgkm_wgkm_{t}_test85.explain{lm}.txt.gz"))
+    got = _np(gk.gkmexplain(m, seqs, mode=mode))
+    np.testing.assert_allclose(got, want, rtol=2e-5, atol=5e-6 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("kind", ["est", "rbf"])
+def test_lsgkm_mutation_impact(kind):
+    m = gk.load_lsgkm_model(os.path.join(LSGKM, f"lsgkm_mode5_{kind}.model.txt.gz")).cuda()
+    _, seqs = read_fasta(os.path.join(LSGKM, "lsgkm_mode5_test51.fa"))
+    rows = [line.split("\t") for line in open(os.path.join(LSGKM, f"lsgkm_mode5_{kind}.txt"))]
+    want = np.array([[float(v) for v in r[2].split(",")] for r in rows])
+    c = len(seqs[0]) // 2
+    ref, alt = [], []
+    for s in seqs:
+        for b in "ACGT":
+            ref.append(s)
+            alt.append(s[:c] + b + s[c + 1:])
+    got = _np(gk.mutation_impact(m, ref, alt)).reshape(-1, 4)
+    np.testing.assert_allclose(got, want, rtol=1e-4, atol=1e-6)
 
 
 def test_encode_10sv_gkmpredict():
