@@ -598,6 +598,46 @@ extern "C" int gkm_index_lmer_weights(const gkm_index_t *ix, const double *c_sv,
     return GKM_OK;
 }
 
+__global__ void index_count_kernel(const uint32_t *__restrict__ bx, const int32_t *__restrict__ cx, int64_t B,
+                                   int64_t W, const uint32_t *__restrict__ off, const uint32_t *__restrict__ masks,
+                                   int n_masks, int64_t n_lmers, int tiles, unsigned long long *__restrict__ out)
+{
+    int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long hits = 0, looks = 0;
+    if (idx < B * W) {
+        int64_t b = idx / W;
+        int i = (int)(idx - b * W);
+        if (i < cx[b]) {
+            uint32_t u = bx[idx];
+            looks = n_masks;
+            for (int c = 0; c < n_masks; c++) {
+                uint32_t v = u ^ (__ldg(masks + c) & 0x00FFFFFFu);
+                for (int t = 0; t < tiles; t++) hits += off[t * n_lmers + v + 1] - off[t * n_lmers + v];
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        hits += __shfl_xor_sync(GKM_FULL, hits, o);
+        looks += __shfl_xor_sync(GKM_FULL, looks, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (hits || looks)) {
+        atomicAdd(out, looks);
+        atomicAdd(out + 1, hits);
+    }
+}
+
+extern "C" int gkm_index_count(const gkm_index_t *ix, const uint32_t *bx, const int32_t *cx, int64_t B, int64_t W,
+                               uint64_t *out, gkm_stream_t stream)
+{
+    if (!ix || !bx || !cx || !out) return gkm_fail(GKM_ERR_INVALID, "null argument");
+    int64_t n = B * W;
+    if (n == 0) return GKM_OK;
+    index_count_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        bx, cx, B, W, ix->offsets, ix->masks, ix->n_masks, ix->n_lmers, ix->tiles, (unsigned long long *)out);
+    GKM_CHECK_LAUNCH("index_count");
+    return GKM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // ISM through the index (kernels/lmer_index_cpu.py:203-285): per (position p,
 // row b), the windows covering p before (set 0) and after each substitution v

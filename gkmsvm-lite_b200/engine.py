@@ -62,7 +62,9 @@ def pack(spec: Spec, codes: torch.Tensor, lengths) -> tuple:
     rc = torch.empty((B, W), dtype=U32, device=dev) if spec.base.include_rc else None
     counts = torch.empty(B, dtype=torch.int32, device=dev)
     ln = None
-    if lengths is not None:
+    if isinstance(lengths, torch.Tensor):
+        ln = lengths.to(device=dev, dtype=torch.int64)
+    elif lengths is not None:
         ln = torch.as_tensor(np.asarray(lengths, dtype=np.int64)).to(dev, non_blocking=True)
     call("gkm_pack", spec.ref, ptr(codes), ptr(ln), B, L, ptr(fwd), ptr(rc), ptr(counts), _st())
     return fwd, rc, counts
@@ -134,6 +136,12 @@ class DeviceIndex:
         call("gkm_index_score", self.handle, ptr(bx), ptr(cx), B, W, ptr(inv_dx), ptr(inv_ds), ptr(coef),
              float(gamma), int(rbf), float(bias), ptr(order), ptr(out), _st())
         return out
+
+    def count(self, bx, cx):
+        """(lookups, hits) an index query over rows bx makes."""
+        out = torch.zeros(2, dtype=torch.int64, device=bx.device)
+        call("gkm_index_count", self.handle, ptr(bx), ptr(cx), bx.shape[0], bx.shape[1], ptr(out), _st())
+        return [int(v) for v in out.cpu()]
 
     def lmer_weights(self, c_sv):
         n = 4**self.spec.base.l

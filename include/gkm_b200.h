@@ -111,6 +111,13 @@ int gkm_index_score(const gkm_index_t *index, const uint32_t *bx, const int32_t 
                     const double *coef, double gamma, int32_t rbf, double bias,
                     const int32_t *order, double *scores, gkm_stream_t stream);
 
+/* Work counts of an index query over rows bx: lookups (query windows x
+ * neighbour masks) and hits (index entries those lookups visit, all tiles);
+ * out [2] uint64, accumulated.  Used to state the algorithmic bytes of a
+ * query (kernels/lmer_index_cpu.py:23-37 visits the same). */
+int gkm_index_count(const gkm_index_t *index, const uint32_t *bx, const int32_t *cx,
+                    int64_t B, int64_t W, uint64_t *out, gkm_stream_t stream);
+
 /* V[v] = sum over index entries of l-mer v of c_sv[sv] times the entry's
  * window weight, [4^l].
  * Replaces sv_lmer_weights (lmer_table.py:35-55). */

@@ -553,7 +553,7 @@ class IndexBaseline:
     CSR over the SVs' windows (kernels/lmer_index.py:161-200) and the fused
     query + reduce (kernels/lmer_index_cpu.py:71-120)."""
 
-    def __init__(self, model: OracleModel):
+    def __init__(self, model: OracleModel, sv_diag=None):
         kd = model.kd
         self.kd = kd
         self.model = model
@@ -572,7 +572,8 @@ class IndexBaseline:
                                        _p(ws), _p(wr), S, W, kd.l)
         self.masks, lev = neighbor_masks(kd.l, kd.h, kd.dmax)
         self.weights = kd.h[lev].astype(np.float64)
-        ds = raw_from_profiles(self_profiles(model.sv, model.sv_lengths, kd), kd)
+        ds = sv_diag if sv_diag is not None else raw_from_profiles(
+            self_profiles(model.sv, model.sv_lengths, kd), kd)
         self.inv_ds = 1.0 / np.sqrt(np.clip(ds, 1e-20, None))
 
     def __del__(self):
