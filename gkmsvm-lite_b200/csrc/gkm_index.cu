@@ -769,3 +769,77 @@ extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, con
     return s;
 }
 
+
+// ---------------------------------------------------------------------------
+// gkm_index_score_noalloc: the same scores as gkm_index_score for callers that
+// must not allocate device memory while they run -- an application that owns
+// the whole device heap through its own pool, a real-time serving loop that
+// may not block in the allocator, or code that calls in from a context where
+// cudaMalloc is forbidden.  The per-(row, SV tile) partial sums that
+// gkm_index_score allocates per call live instead in the fixed array below,
+// which every device that loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+
+#include <mutex>
+
+#define GKM_NOALLOC_MAX_PARTIALS (1 << 19)  // rows x SV tiles per call: 4 MiB of doubles
+#define GKM_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) double g_noalloc_partials[GKM_NOALLOC_MAX_PARTIALS];
+
+// Device address of g_noalloc_partials on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, once per device (with that device current), cached.
+static int noalloc_partials(double **out)
+{
+    static std::mutex mu;
+    static double *addr[GKM_NOALLOC_MAX_DEVICES] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return gkm_cuda_status(e, "gkm_index_score_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= GKM_NOALLOC_MAX_DEVICES)
+        return gkm_fail(GKM_ERR_UNSUPPORTED, "gkm_index_score_noalloc: device %d beyond %d", dev,
+                        GKM_NOALLOC_MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess) return gkm_cuda_status(e, "gkm_index_score_noalloc: cudaGetSymbolAddress");
+        addr[dev] = (double *)p;
+    }
+    *out = addr[dev];
+    return GKM_OK;
+}
+
+extern "C" int gkm_index_score_noalloc(const gkm_index_t *ix, const uint32_t *bx, const int32_t *cx, int64_t B,
+                                       int64_t W, const double *inv_dx, const double *inv_ds, const double *coef,
+                                       double gamma, int32_t rbf, double bias, const int32_t *order,
+                                       double *scores, gkm_stream_t stream)
+{
+    if (!ix || !bx || !cx || !inv_dx || !inv_ds || !coef || !scores)
+        return gkm_fail(GKM_ERR_INVALID, "null argument");
+    if (B == 0) return GKM_OK;
+    if (B * (int64_t)ix->tiles > GKM_NOALLOC_MAX_PARTIALS)
+        return gkm_fail(GKM_ERR_CAPACITY,
+                        "gkm_index_score_noalloc: %lld rows x %d SV tiles exceed its fixed scratch of %d "
+                        "partial sums; score at most %lld rows per call",
+                        (long long)B, ix->tiles, GKM_NOALLOC_MAX_PARTIALS,
+                        (long long)(GKM_NOALLOC_MAX_PARTIALS / ix->tiles));
+    double *partial = nullptr;
+    GKM_TRY(noalloc_partials(&partial));
+    cudaStream_t st = (cudaStream_t)stream;
+    // Every (row, tile) partial is written before finish_scores reads it, so
+    // nothing in the scratch has to start at zero.
+    QueryArgs a = query_args(ix, bx, cx, W);
+    a.order = order;
+    a.inv_dx = inv_dx;
+    a.inv_ds = inv_ds;
+    a.coef = coef;
+    a.gamma = gamma;
+    a.rbf = rbf;
+    a.partial = partial;
+    GKM_TRY(query_launch<MODE_SCORE>(ix, a, B, st));
+    finish_scores<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(partial, B, ix->tiles, bias, scores);
+    GKM_CHECK_LAUNCH("finish_scores");
+    return GKM_OK;
+}

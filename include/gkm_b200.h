@@ -111,6 +111,21 @@ int gkm_index_score(const gkm_index_t *index, const uint32_t *bx, const int32_t 
                     const double *coef, double gamma, int32_t rbf, double bias,
                     const int32_t *order, double *scores, gkm_stream_t stream);
 
+/* gkm_index_score without any device allocation, for callers that cannot
+ * allocate while scoring (a process whose device heap is owned by its own
+ * pool, a serving loop that must not block in the allocator).  No counterpart
+ * in gkmsvm-lite.  Its per-(row, SV tile) partial sums live in one fixed
+ * 4 MiB device array that the library holds on every device it is loaded on
+ * until exit, so B x tiles must be <= 524,288 (GKM_ERR_CAPACITY otherwise).
+ * The first call on a device looks that array's address up
+ * (cudaGetSymbolAddress): make it before any stream capture.  All calls share
+ * the array, so calls that overlap on the GPU (other streams, other threads)
+ * race; serialise them. */
+int gkm_index_score_noalloc(const gkm_index_t *index, const uint32_t *bx, const int32_t *cx,
+                            int64_t B, int64_t W, const double *inv_dx, const double *inv_ds,
+                            const double *coef, double gamma, int32_t rbf, double bias,
+                            const int32_t *order, double *scores, gkm_stream_t stream);
+
 /* Work counts of an index query over rows bx: lookups (query windows x
  * neighbour masks) and hits (index entries those lookups visit, all tiles);
  * out [2] uint64, accumulated.  Used to state the algorithmic bytes of a
