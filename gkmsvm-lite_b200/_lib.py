@@ -54,6 +54,7 @@ SIGNATURES = {
     "gkm_index_create": [SPEC, P, P, P, I64, I64, P, I32, I32, P, P],
     "gkm_index_free": [P],
     "gkm_index_info": [P, P, P, P, P],
+    "gkm_index_status": [P, P, I32, P],
     "gkm_index_pairwise": [P, P, P, I64, I64, I64, P, P, P],
     "gkm_index_score": [P, P, P, I64, I64, P, P, P, D, I32, D, P, P, P],
     "gkm_index_lmer_weights": [P, P, P, P],

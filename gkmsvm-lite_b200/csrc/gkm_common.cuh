@@ -108,10 +108,14 @@ struct gkm_index {
     int64_t n_lmers;     // 4^l
     int64_t entries;     // indexed windows
     uint32_t *offsets;   // [tiles * n_lmers + 1] start of bucket (tile, v)
-    uint32_t *ent;       // [entries] local SV id (bits 0..23) | weight << 24
+    uint32_t *ent;       // [entries] local SV id (bits 0..23) | weight << 24 (weighted, or big tiles)
+    uint16_t *ent16;     // [entries] local SV id (unweighted tiles of <= 65,536 SVs), else null
     uint32_t *masks;     // [n_masks] mask | level << 24
     int32_t n_masks;
     int64_t bytes;
+    int32_t acc_bytes;   // shared memory left for counters in a query block
+    int32_t wide;        // 1: 32-bit counters (weighted, or after a carry-log overflow)
+    int *status;         // device flags set by queries (see gkm_index_status)
 };
 
 int gkm_smem_limit();

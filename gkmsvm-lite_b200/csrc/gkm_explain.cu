@@ -29,6 +29,7 @@ struct ExplainArgs {
     // index path
     const uint32_t *off;
     const uint32_t *ent;
+    const uint16_t *ent16;
     int tiles;
     int tile_svs;
     int64_t n_lmers;
@@ -77,7 +78,7 @@ __global__ void __launch_bounds__(EX_WARPS * 32) explain_windows(ExplainArgs a)
                 const uint32_t e0 = __ldg(o + v), e1 = __ldg(o + v + 1);
                 const double *wt = wrow + (int64_t)t * a.tile_svs;
                 for (uint32_t e = e0; e < e1; e++) {
-                    const uint32_t en = __ldg(a.ent + e);
+                    const uint32_t en = a.ent16 ? (uint32_t)__ldg(a.ent16 + e) | (1u << 24) : __ldg(a.ent + e);
                     double x = __ldg(wt + (en & 0x00FFFFFFu));
                     val += a.weighted ? x * (double)(en >> 24) : x;
                 }
@@ -168,6 +169,7 @@ extern "C" int gkm_explain_lmer(const gkm_spec *spec, const uint32_t *fwd, const
     if (!V) {
         a.off = index->offsets;
         a.ent = index->ent;
+        a.ent16 = index->ent16;
         a.tiles = index->tiles;
         a.tile_svs = index->tile_svs;
         a.n_lmers = index->n_lmers;

@@ -235,6 +235,12 @@ __global__ void entry_gen(gkm_spec spec, const uint32_t *__restrict__ fwd, const
     }
 }
 
+__global__ void narrow_entries(const uint32_t *__restrict__ vals, int64_t n, uint16_t *__restrict__ out)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (uint16_t)(vals[i] & 0xFFFFu);
+}
+
 __global__ void bucket_offsets(const uint32_t *__restrict__ keys, int64_t E, int64_t nbuckets,
                                uint32_t *__restrict__ off)
 {
@@ -250,7 +256,11 @@ __global__ void bucket_offsets(const uint32_t *__restrict__ keys, int64_t E, int
 // ---------------------------------------------------------------------------
 
 constexpr int Q_THREADS = 1024;
+constexpr int Q_WARPS = Q_THREADS / 32;
+constexpr int LOG_CAP = 64;            // carry events a block can log (16-bit counters)
+constexpr int MASKS_SMEM_MAX = 6144;   // neighbour masks staged in shared memory up to this
 enum { MODE_SCORE = 0, MODE_RAW = 1 };
+enum { EV_LOWCARRY = 0, EV_WRAP = 1 };
 
 struct QueryArgs {
     const uint32_t *bx;
@@ -260,17 +270,19 @@ struct QueryArgs {
     int64_t diag_offset;  // >= 0: row r is column diag_offset + r
     // index
     const uint32_t *off;
-    const uint32_t *ent;
+    const void *ent;      // uint16 local ids, or uint32 id | weight << 24
     const uint32_t *masks;
     int n_masks;
     int64_t n_lmers;
     int64_t S;
     int tile_svs;
+    int sub_svs;          // SVs per accumulation pass (wide counters)
     int nlev;
     int dmax;
     double h[16];
     const uint8_t *wd;
     const uint8_t *wq;    // [rows, W] query window weights (null: from the row's count)
+    int *status;          // bit 0: a block's carry log overflowed; bit 1: a wide counter wrapped
     // score
     const double *inv_dx;
     const double *inv_ds;
@@ -284,59 +296,193 @@ struct QueryArgs {
     int l;
 };
 
-template <bool WEIGHTED, int MODE>
-__global__ void __launch_bounds__(Q_THREADS) index_query(QueryArgs a)
+// Shared memory of a query block: staged masks and the carry log, then the
+// counters.
+__host__ __device__ inline size_t query_fixed_smem(int n_masks)
 {
-    extern __shared__ uint32_t acc[];  // [nlev][tile_svs]
+    size_t m = n_masks <= MASKS_SMEM_MAX ? (size_t)n_masks * 4 : 0;
+    m = (m + 15) & ~(size_t)15;
+    return m + LOG_CAP * 4 + 64;
+}
+
+// C16: unweighted pair counts in 16-bit fields, two SVs of one level per
+// 32-bit word.  A field that passes 65535 carries into its neighbour (or out
+// of the word); the adder sees that in the value atomicAdd returns and logs
+// it, and the epilogue adds the carries back, so the counts stay exact.
+template <bool C16>
+__device__ __forceinline__ int64_t read_count(const uint32_t *acc, const uint32_t *log, int nlog, int m, int St,
+                                              int s)
+{
+    if (!C16) return acc[m * St + s];
+    // levels 2j and 2j+1 of SV s share word j * St + s (low and high half)
+    const uint32_t word = (uint32_t)((m >> 1) * St + s), half = (uint32_t)(m & 1);
+    int64_t f = (acc[word] >> (16 * half)) & 0xFFFFu;
+    for (int e = 0; e < nlog; e++) {
+        uint32_t ev = log[e];
+        if ((ev >> 1) != word) continue;
+        if ((ev & 1u) == EV_LOWCARRY)
+            f += half ? -1 : 65536;
+        else if (half)
+            f += 65536;
+    }
+    return f;
+}
+
+// C16 counter update: add (1 << 16 * half) to word; fmask selects the field.
+__device__ __forceinline__ void count16(uint32_t *acc, uint32_t word, uint32_t add, uint32_t fmask, int *nlog,
+                                        uint32_t *log, int *status)
+{
+    const uint32_t old = atomicAdd(acc + word, add);
+    if ((old & fmask) == fmask) {  // the field was 0xFFFF: it carries
+        const bool low = fmask == 0xFFFFu;
+        const int p0 = atomicAdd(nlog, (low && old == 0xFFFFFFFFu) ? 2 : 1);
+        if (p0 + 1 < LOG_CAP) {
+            if (!low) {
+                log[p0] = (word << 1) | EV_WRAP;
+            } else {
+                log[p0] = (word << 1) | EV_LOWCARRY;
+                if (old == 0xFFFFFFFFu) log[p0 + 1] = (word << 1) | EV_WRAP;
+            }
+        } else {
+            atomicOr(status, 1);
+        }
+    }
+}
+
+// Index entry k: 16-bit local SV id (unweighted tiles of <= 65,536 SVs), or
+// local id | window weight << 24.
+template <bool E16>
+__device__ __forceinline__ uint32_t load_entry(const void *ent, uint32_t k)
+{
+    if (E16) return (uint32_t)__ldg((const uint16_t *)ent + k);
+    return __ldg((const uint32_t *)ent + k);
+}
+
+// One block per (row, SV tile): each warp takes whole query windows; each
+// lane one neighbour mask per chunk of 32, scanning its bucket four entries
+// at a time (the four loads in flight together); the next chunk's bucket
+// bounds are loaded while this chunk's entries are counted.
+template <bool WEIGHTED, int MODE, bool C16, bool E16, bool RANGE>
+__global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
+{
+    extern __shared__ __align__(16) uint8_t smraw[];
     __shared__ double red[32];
+    __shared__ int nlog;
+    const int n_masks = a.n_masks;
+    uint32_t *sm_masks = n_masks <= MASKS_SMEM_MAX ? (uint32_t *)smraw : nullptr;
+    uint32_t *sm_log = (uint32_t *)(smraw + ((sm_masks ? (size_t)n_masks * 4 : 0) + 15 & ~(size_t)15));
+    uint32_t *sm_acc = (uint32_t *)(smraw + query_fixed_smem(n_masks));
     const int64_t r = blockIdx.x;
     const int64_t row = a.order ? a.order[r] : r;
     const int t = blockIdx.y;
     const int St = a.tile_svs;
     const int64_t s0 = (int64_t)t * St;
     const int ns = (int)min((int64_t)St, a.S - s0);
-    int64_t lo_g = a.diag_offset >= 0 ? a.diag_offset + row : 0;
+    const int64_t lo_g = a.diag_offset >= 0 ? a.diag_offset + row : 0;
     if (MODE == MODE_RAW && s0 + ns <= lo_g) return;  // tile wholly below the diagonal
     const uint32_t lo = (uint32_t)(lo_g > s0 ? lo_g - s0 : 0);
-    const int nacc = a.nlev * St;
-    for (int k = threadIdx.x; k < nacc; k += Q_THREADS) acc[k] = 0;
-    __syncthreads();
+    if (sm_masks)
+        for (int k = threadIdx.x; k < n_masks; k += Q_THREADS) sm_masks[k] = a.masks[k];
+    const uint32_t *masks = sm_masks ? sm_masks : a.masks;
     const int n = a.cx[row];
     const uint32_t *x = a.bx + row * a.W;
     const uint32_t *off = a.off + (int64_t)t * a.n_lmers;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = warp; i < n; i += Q_THREADS / 32) {
-        const uint32_t u = x[i];
-        const uint32_t wq = WEIGHTED ? (a.wq ? (uint32_t)a.wq[row * a.W + i] : gkm_wt(a.wd, n, i)) : 1u;
-        for (int c = lane; c < a.n_masks; c += 32) {
-            const uint32_t mk = __ldg(a.masks + c);
-            const uint32_t v = u ^ (mk & 0x00FFFFFFu);
-            uint32_t *lev = acc + (mk >> 24) * St;
-            const uint32_t beg = __ldg(off + v), end = __ldg(off + v + 1);
-            for (uint32_t e = end; e > beg; e--) {
-                const uint32_t en = __ldg(a.ent + e - 1);
-                const uint32_t id = en & 0x00FFFFFFu;
-                if (id < lo) break;  // bucket ids ascend
-                atomicAdd(lev + id, WEIGHTED ? wq * (en >> 24) : 1u);
-            }
-        }
-    }
-    __syncthreads();
+    const double inv_dx = MODE == MODE_SCORE ? a.inv_dx[row] : 0.0;
     double part = 0.0;
-    for (int s = threadIdx.x; s < ns; s += Q_THREADS) {
-        double k = 0.0;
-        for (int m = 0; m < a.nlev; m++) k += a.h[m] * (double)acc[m * St + s];
-        const int64_t sg = s0 + s;
-        if (MODE == MODE_SCORE) {
-            double kn = k * a.inv_dx[row] * a.inv_ds[sg];
-            part += a.coef[sg] * (a.rbf ? exp(a.gamma * (kn - 1.0)) : kn);
-        } else if (s >= (int)lo) {
-            if (a.raw) a.raw[row * a.S + sg] = k;
-            if (a.profile) {
-                uint64_t *p = a.profile + (row * a.S + sg) * (a.l + 1);
-                for (int m = 0; m <= a.l; m++) p[m] = m < a.nlev ? acc[m * St + s] : 0;
+    const int sub = C16 ? ns : a.sub_svs;
+    for (int sub_lo = 0; sub_lo < ns; sub_lo += sub) {
+        const int sub_n = min(sub, ns - sub_lo);
+        const int stride = C16 ? St : sub_n;
+        const int nacc = C16 ? ((a.nlev + 1) / 2) * St : a.nlev * sub_n;
+        for (int k = threadIdx.x; k < nacc; k += Q_THREADS) sm_acc[k] = 0;
+        if (threadIdx.x == 0) nlog = 0;
+        __syncthreads();
+        const uint32_t id_lo = max((uint32_t)sub_lo, lo), id_hi = (uint32_t)(sub_lo + sub_n);
+        for (int i = warp; i < n; i += Q_WARPS) {
+            const uint32_t u = x[i];
+            const uint32_t wq = WEIGHTED ? (a.wq ? (uint32_t)a.wq[row * a.W + i] : gkm_wt(a.wd, n, i)) : 1u;
+            // per lane: its mask's bucket and counter slot (C16: word base and
+            // field of the level; wide: row base of the level)
+            uint32_t beg = 0, end = 0, base = 0, add = 0, fmask = 0;
+            auto lane_mask = [&](int c, uint32_t &b0, uint32_t &e0, uint32_t &bs, uint32_t &ad, uint32_t &fm) {
+                const uint32_t mk = masks[c];
+                const uint32_t v = u ^ (mk & 0x00FFFFFFu);
+                const uint32_t lev = mk >> 24;
+                if (C16) {
+                    bs = (lev >> 1) * (uint32_t)St;
+                    ad = 1u << (16 * (lev & 1u));
+                    fm = 0xFFFFu << (16 * (lev & 1u));
+                } else {
+                    bs = lev * (uint32_t)stride - (uint32_t)sub_lo;
+                }
+                b0 = __ldg(off + v);
+                e0 = __ldg(off + v + 1);
+            };
+            if (lane < n_masks) lane_mask(lane, beg, end, base, add, fmask);
+            for (int c0 = 0; c0 < n_masks; c0 += 32) {
+                uint32_t nbeg = 0, nend = 0, nbase = 0, nadd = 0, nfm = 0;
+                const int cn = c0 + 32 + lane;
+                if (cn < n_masks) lane_mask(cn, nbeg, nend, nbase, nadd, nfm);
+                // the bucket in aligned blocks of four entries, one vector load each
+                for (uint32_t e = beg & ~3u; __any_sync(GKM_FULL, e < end); e += 4) {
+                    uint32_t en[4];
+                    if (e < end) {
+                        if (E16) {
+                            const uint2 w = __ldg((const uint2 *)((const uint16_t *)a.ent + e));
+                            en[0] = w.x & 0xFFFFu;
+                            en[1] = w.x >> 16;
+                            en[2] = w.y & 0xFFFFu;
+                            en[3] = w.y >> 16;
+                        } else {
+                            const uint4 w = __ldg((const uint4 *)((const uint32_t *)a.ent + e));
+                            en[0] = w.x;
+                            en[1] = w.y;
+                            en[2] = w.z;
+                            en[3] = w.w;
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        if (e + q < beg || e + q >= end) continue;
+                        const uint32_t id = E16 ? en[q] : (en[q] & 0x00FFFFFFu);
+                        if (RANGE && (id < id_lo || id >= id_hi)) continue;
+                        if (C16)
+                            count16(sm_acc, base + id, add, fmask, &nlog, sm_log, a.status);
+                        else {
+                            const uint32_t inc = WEIGHTED ? wq * (en[q] >> 24) : 1u;
+                            const uint32_t old = atomicAdd(sm_acc + base + id, inc);
+                            if (old + inc < old) atomicOr(a.status, 2);
+                        }
+                    }
+                }
+                beg = nbeg;
+                end = nend;
+                base = nbase;
+                add = nadd;
+                fmask = nfm;
             }
         }
+        __syncthreads();
+        const int nl = min(nlog, LOG_CAP);
+        for (int s = sub_lo + threadIdx.x; s < sub_lo + sub_n; s += Q_THREADS) {
+            double k = 0.0;
+            for (int m = 0; m < a.nlev; m++)
+                k += a.h[m] * (double)read_count<C16>(sm_acc, sm_log, nl, m, stride, s - sub_lo);
+            const int64_t sg = s0 + s;
+            if (MODE == MODE_SCORE) {
+                const double kn = k * inv_dx * a.inv_ds[sg];
+                part += a.coef[sg] * (a.rbf ? exp(a.gamma * (kn - 1.0)) : kn);
+            } else if (s >= (int)lo) {
+                if (a.raw) a.raw[row * a.S + sg] = k;
+                if (a.profile) {
+                    uint64_t *pp = a.profile + (row * a.S + sg) * (a.l + 1);
+                    for (int m = 0; m <= a.l; m++)
+                        pp[m] = m < a.nlev ? (uint64_t)read_count<C16>(sm_acc, sm_log, nl, m, stride, s - sub_lo) : 0;
+                }
+            }
+        }
+        __syncthreads();
     }
     if (MODE == MODE_SCORE) {
         part = gkm_block_sum(part, red);
@@ -356,8 +502,8 @@ __global__ void finish_scores(const double *__restrict__ partial, int64_t B, int
 
 // V[v] over every tile's bucket of v (lmer_table.py:35-55)
 __global__ void lmer_weights_kernel(const uint32_t *__restrict__ off, const uint32_t *__restrict__ ent,
-                                    int64_t n_lmers, int tiles, int tile_svs, int weighted,
-                                    const double *__restrict__ c_sv, double *__restrict__ V)
+                                    const uint16_t *__restrict__ ent16, int64_t n_lmers, int tiles, int tile_svs,
+                                    int weighted, const double *__restrict__ c_sv, double *__restrict__ V)
 {
     int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n_lmers) return;
@@ -365,7 +511,7 @@ __global__ void lmer_weights_kernel(const uint32_t *__restrict__ off, const uint
     for (int t = 0; t < tiles; t++) {
         uint32_t b = off[t * n_lmers + v], e = off[t * n_lmers + v + 1];
         for (uint32_t k = b; k < e; k++) {
-            uint32_t en = ent[k];
+            uint32_t en = ent16 ? (uint32_t)ent16[k] | (1u << 24) : ent[k];
             double c = c_sv[(int64_t)t * tile_svs + (en & 0x00FFFFFFu)];
             acc += weighted ? c * (double)(en >> 24) : c;
         }
@@ -404,13 +550,19 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
     if (spec->weighted && !spec->wd) return gkm_fail(GKM_ERR_INVALID, "weighted spec without weights");
     cudaStream_t st = (cudaStream_t)stream;
     int nlev = spec->dmax + 1;
-    int smem = gkm_smem_limit() - 1024;
-    int max_tile = smem / (4 * nlev);
+    // counter bytes per SV: 16-bit fields (unweighted) or 32-bit (weighted)
+    int acc_bytes = gkm_smem_limit() - 1024 - (int)query_fixed_smem(n_masks);
+    // 16-bit counters pack two levels of an SV per 32-bit word
+    int per_sv = spec->weighted ? 4 * nlev : 4 * ((nlev + 1) / 2);
+    int max_tile = (acc_bytes / per_sv) & ~1;
+    if (max_tile < 2) return gkm_fail(GKM_ERR_UNSUPPORTED, "%d mismatch levels do not fit shared memory", nlev);
     if (tile_svs <= 0) {
         int64_t T = (S + max_tile - 1) / max_tile;
         tile_svs = (int32_t)((S + T - 1) / T);
+        tile_svs += tile_svs & 1;
     }
     if (tile_svs > max_tile || tile_svs > (1 << 24)) return gkm_fail(GKM_ERR_INVALID, "tile_svs %d too large", tile_svs);
+    if (tile_svs & 1) tile_svs++;
     int64_t T = (S + tile_svs - 1) / tile_svs;
     int tile_bits = 0;
     while ((1LL << tile_bits) < T) tile_bits++;
@@ -426,6 +578,8 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
     ix->nlev = nlev;
     ix->n_lmers = (int64_t)1 << (2 * spec->l);
     ix->n_masks = n_masks;
+    ix->acc_bytes = acc_bytes;
+    ix->wide = spec->weighted ? 1 : 0;
     int status = GKM_OK;
     uint32_t *ecount = nullptr, *base = nullptr, *keys = nullptr, *vals = nullptr, *kt = nullptr, *vt = nullptr;
     uint32_t total = 0;
@@ -461,12 +615,27 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
         }
         bucket_offsets<<<(unsigned)((total + 1 + 255) / 256), 256, 0, st>>>(keys, total, nbuckets, ix->offsets);
         GKM_CHECK_LAUNCH("bucket_offsets");
-        if (cudaMalloc(&ix->ent, eb) != cudaSuccess || cudaMalloc(&ix->masks, sizeof(uint32_t) * n_masks) != cudaSuccess) {
+        bool compact = !spec->weighted && tile_svs <= 65536;
+        // queries read entries in aligned blocks of four: pad the arrays by a block
+        size_t eb16 = sizeof(uint16_t) * ((size_t)total + 8);
+        eb = sizeof(uint32_t) * ((size_t)total + 8);
+        if ((compact ? cudaMalloc(&ix->ent16, eb16) : cudaMalloc(&ix->ent, eb)) != cudaSuccess ||
+            cudaMalloc(&ix->masks, sizeof(uint32_t) * n_masks) != cudaSuccess ||
+            cudaMalloc(&ix->status, sizeof(int)) != cudaSuccess) {
             status = gkm_fail(GKM_ERR_OOM, "index entries");
             break;
         }
-        cudaMemcpyAsync(ix->ent, vals, eb, cudaMemcpyDeviceToDevice, st);
+        if (compact) {
+            cudaMemsetAsync(ix->ent16, 0, eb16, st);
+            narrow_entries<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(vals, total, ix->ent16);
+            GKM_CHECK_LAUNCH("narrow_entries");
+            eb = eb16;
+        } else {
+            cudaMemsetAsync(ix->ent, 0, eb, st);
+            cudaMemcpyAsync(ix->ent, vals, sizeof(uint32_t) * (size_t)total, cudaMemcpyDeviceToDevice, st);
+        }
         cudaMemcpyAsync(ix->masks, masks, sizeof(uint32_t) * n_masks, cudaMemcpyDeviceToDevice, st);
+        cudaMemsetAsync(ix->status, 0, sizeof(int), st);
         ix->bytes = (int64_t)sizeof(uint32_t) * (nbuckets + 1) + (int64_t)eb + sizeof(uint32_t) * n_masks;
     } while (0);
     cudaFreeAsync(ecount, st);
@@ -491,8 +660,26 @@ extern "C" int gkm_index_free(gkm_index_t *ix)
     if (!ix) return GKM_OK;
     cudaFree(ix->offsets);
     cudaFree(ix->ent);
+    cudaFree(ix->ent16);
     cudaFree(ix->masks);
+    cudaFree(ix->status);
     delete ix;
+    return GKM_OK;
+}
+
+extern "C" int gkm_index_status(gkm_index_t *ix, int32_t *flags, int32_t wide, gkm_stream_t stream)
+{
+    if (!ix) return gkm_fail(GKM_ERR_INVALID, "null index");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (flags) {
+        int v = 0;
+        cudaError_t e = cudaMemcpyAsync(&v, ix->status, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return gkm_cuda_status(e, "index status");
+        *flags = v;
+        if (v) cudaMemsetAsync(ix->status, 0, sizeof(int), st);
+    }
+    if (wide >= 0) ix->wide = ix->spec.weighted ? 1 : wide;
     return GKM_OK;
 }
 
@@ -515,12 +702,14 @@ static QueryArgs query_args(const gkm_index_t *ix, const uint32_t *bx, const int
     a.W = W;
     a.diag_offset = -1;
     a.off = ix->offsets;
-    a.ent = ix->ent;
+    a.ent = ix->ent16 ? (const void *)ix->ent16 : (const void *)ix->ent;
     a.masks = ix->masks;
     a.n_masks = ix->n_masks;
     a.n_lmers = ix->n_lmers;
     a.S = ix->S;
     a.tile_svs = ix->tile_svs;
+    a.sub_svs = ix->acc_bytes / (4 * ix->nlev);
+    a.status = ix->status;
     a.nlev = ix->nlev;
     a.dmax = ix->spec.dmax;
     for (int m = 0; m < 16; m++) a.h[m] = ix->spec.h[m];
@@ -529,18 +718,37 @@ static QueryArgs query_args(const gkm_index_t *ix, const uint32_t *bx, const int
     return a;
 }
 
+template <bool WEIGHTED, int MODE, bool C16, bool E16>
+static void launch_query(dim3 grid, size_t smem, cudaStream_t st, const QueryArgs &a)
+{
+    // ids need a range test only for a self-Gram's diagonal or wide sub-ranges
+    if (C16 && a.diag_offset < 0) {
+        cudaFuncSetAttribute(index_query<WEIGHTED, MODE, C16, E16, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        index_query<WEIGHTED, MODE, C16, E16, false><<<grid, Q_THREADS, smem, st>>>(a);
+    } else {
+        cudaFuncSetAttribute(index_query<WEIGHTED, MODE, C16, E16, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        index_query<WEIGHTED, MODE, C16, E16, true><<<grid, Q_THREADS, smem, st>>>(a);
+    }
+}
+
 template <int MODE>
 static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cudaStream_t st)
 {
-    size_t smem = sizeof(uint32_t) * (size_t)ix->nlev * ix->tile_svs;
+    if (B > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many rows for one launch");
+    size_t smem = query_fixed_smem(ix->n_masks) + 16 + (size_t)ix->acc_bytes;
     dim3 grid((unsigned)B, (unsigned)ix->tiles);
-    if (ix->spec.weighted) {
-        cudaFuncSetAttribute(index_query<true, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        index_query<true, MODE><<<grid, Q_THREADS, smem, st>>>(a);
-    } else {
-        cudaFuncSetAttribute(index_query<false, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        index_query<false, MODE><<<grid, Q_THREADS, smem, st>>>(a);
-    }
+    if (ix->spec.weighted)
+        launch_query<true, MODE, false, false>(grid, smem, st, a);
+    else if (ix->ent16 && ix->wide)
+        launch_query<false, MODE, false, true>(grid, smem, st, a);
+    else if (ix->ent16)
+        launch_query<false, MODE, true, true>(grid, smem, st, a);
+    else if (ix->wide)
+        launch_query<false, MODE, false, false>(grid, smem, st, a);
+    else
+        launch_query<false, MODE, true, false>(grid, smem, st, a);
     GKM_CHECK_LAUNCH("index_query");
     return GKM_OK;
 }
@@ -593,7 +801,7 @@ extern "C" int gkm_index_lmer_weights(const gkm_index_t *ix, const double *c_sv,
     if (!ix || !c_sv || !V) return gkm_fail(GKM_ERR_INVALID, "null argument");
     int64_t n = ix->n_lmers;
     lmer_weights_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-        ix->offsets, ix->ent, n, ix->tiles, ix->tile_svs, ix->spec.weighted, c_sv, V);
+        ix->offsets, ix->ent, ix->ent16, n, ix->tiles, ix->tile_svs, ix->spec.weighted, c_sv, V);
     GKM_CHECK_LAUNCH("lmer_weights");
     return GKM_OK;
 }

@@ -119,23 +119,57 @@ class DeviceIndex:
         except Exception:
             pass
 
+    def flags(self) -> int:
+        """Query flags since the last read (synchronises the stream)."""
+        f = ctypes.c_int32()
+        call("gkm_index_status", self.handle, ctypes.byref(f), -1, _st())
+        return f.value
+
+    def set_wide(self, wide: bool) -> None:
+        call("gkm_index_status", self.handle, None, int(bool(wide)), _st())
+
+    def checked(self, run):
+        """run() through the index; when a query block's 16-bit counters
+        carried more often than its log holds, run it again with 32-bit
+        counters (exact either way); a wrapped 32-bit counter raises."""
+        out = run()
+        f = self.flags()
+        if f & 1:
+            self.set_wide(True)
+            try:
+                out = run()
+                f = self.flags()
+            finally:
+                self.set_wide(False)
+        if f & 2:
+            raise _lib.GkmError(_lib.GKM_ERR_CAPACITY, "a weighted pair count passed 2^32 for one (row, SV) pair")
+        return out
+
     def pairwise(self, bx, cx, diag_offset=None, raw=True, profile=False, out=None):
         B, W = bx.shape
         if raw and out is None:
             out = torch.zeros((B, self.S), dtype=torch.float64, device=bx.device)
         prof = (torch.zeros((B, self.S, self.spec.base.l + 1), dtype=torch.int64, device=bx.device)
                 if profile else None)
-        call("gkm_index_pairwise", self.handle, ptr(bx), ptr(cx), B, W,
-             -1 if diag_offset is None else int(diag_offset), ptr(out if raw else None), ptr(prof), _st())
-        return out, prof
 
-    def score(self, bx, cx, inv_dx, inv_ds, coef, gamma, rbf, bias, order=None, out=None):
+        def run():
+            call("gkm_index_pairwise", self.handle, ptr(bx), ptr(cx), B, W,
+                 -1 if diag_offset is None else int(diag_offset), ptr(out if raw else None), ptr(prof), _st())
+            return out, prof
+
+        return self.checked(run)
+
+    def score(self, bx, cx, inv_dx, inv_ds, coef, gamma, rbf, bias, order=None, out=None, check=True):
         B, W = bx.shape
         if out is None:
             out = torch.empty(B, dtype=torch.float64, device=bx.device)
-        call("gkm_index_score", self.handle, ptr(bx), ptr(cx), B, W, ptr(inv_dx), ptr(inv_ds), ptr(coef),
-             float(gamma), int(rbf), float(bias), ptr(order), ptr(out), _st())
-        return out
+
+        def run():
+            call("gkm_index_score", self.handle, ptr(bx), ptr(cx), B, W, ptr(inv_dx), ptr(inv_ds), ptr(coef),
+                 float(gamma), int(rbf), float(bias), ptr(order), ptr(out), _st())
+            return out
+
+        return self.checked(run) if check else run()
 
     def count(self, bx, cx):
         """(lookups, hits) an index query over rows bx makes."""

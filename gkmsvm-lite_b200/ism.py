@@ -80,7 +80,11 @@ def _ism_index(model, fwd, rc, counts, L):
     ref_raw, _ = index.pairwise(fwd, counts)
     ref_score = index.score(fwd, counts, inv_dx, model._inv_ds(), model._sv_coef(), gamma, rbf, 0.0)
     out = torch.empty((B, 4, L), dtype=torch.float64, device=fwd.device)
-    call("gkm_index_mutants", index.handle, ptr(fwd), ptr(counts), B, W, L, ptr(ref_raw), ptr(ref_score),
-         ptr(inv_dx), ptr(inv_dmut), ptr(model._inv_ds()), ptr(model._sv_coef()), float(gamma), int(rbf),
-         ptr(out), stream_handle())
-    return out
+
+    def run():
+        call("gkm_index_mutants", index.handle, ptr(fwd), ptr(counts), B, W, L, ptr(ref_raw), ptr(ref_score),
+             ptr(inv_dx), ptr(inv_dmut), ptr(model._inv_ds()), ptr(model._sv_coef()), float(gamma), int(rbf),
+             ptr(out), stream_handle())
+        return out
+
+    return index.checked(run)

@@ -314,3 +314,33 @@ def test_encode_10sv_gkmpredict():
         else:
             x = [seq]
         assert abs(float(_np(m(x))[0, 0]) - float(want)) < 1e-4
+
+
+def test_counter_carries_are_exact():
+    """Low-complexity rows push one (row, SV, level) count past 16 bits: the
+    carry log keeps the counts exact, and a block whose carries outgrow the log
+    is rerun with 32-bit counters."""
+    rng = np.random.default_rng(5)
+    sv = np.concatenate([np.zeros((10, 500), np.uint8), rng.integers(0, 4, (30, 500)).astype(np.uint8)])
+    coef = rng.normal(size=40)
+    x = np.concatenate([np.zeros((1, 2000), np.uint8), rng.integers(0, 4, (2, 2000)).astype(np.uint8)])
+    kd = orc.KernelDef.from_params("gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 2.0})
+    want_prof = orc.profiles(x, None, sv, None, kd)
+    assert want_prof[0, 0, 0] > 65535
+    m = gk.GkmSVM(sv, coef, 0.0, "gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 2.0}).cuda()
+    m.use_lmer_table = False
+    index = m._sv_index()
+    spec = m._spec()
+    fwd, rc, counts = engine.pack(spec, torch.from_numpy(x).cuda(), None)
+    # one poly-A SV per tile: carries stay within the log
+    ix1 = engine.DeviceIndex(spec, *m._sv_packed(), m._masks(), tile_svs=2)
+    raw, prof = ix1.pairwise(fwd, counts, profile=True)
+    np.testing.assert_array_equal(_np(prof)[..., :4].astype(np.uint64), want_prof[..., :4])
+    ix1.close()
+    # ten poly-A SVs in one tile: the log overflows and the query reruns
+    inv_dx = 1.0 / torch.sqrt(engine.self_kernel(spec, fwd, rc, counts))
+    index.score(fwd, counts, inv_dx, m._inv_ds(), m._sv_coef(), 2.0, 1, 0.0, check=False)
+    assert index.flags() & 1
+    got = _np(m(x))
+    want = orc.scores(orc.OracleModel(sv, None, coef, 0.0, kd), x)
+    np.testing.assert_allclose(got, want, rtol=RTOL, atol=ATOL)
