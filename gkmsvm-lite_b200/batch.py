@@ -1,0 +1,182 @@
+"""Batched scoring: whole query batches in persistent, CUDA-graph-captured
+launches.
+
+A batch of queries of uneven length is packed into fixed device buffers whose
+shape is rounded up to a bucket (rows to a multiple of 1,024, length to a power
+of two), so a handful of CUDA graphs cover every batch.  Each graph holds the
+whole scoring pass: packing, the query self-kernels, the longest-first row
+order, and the persistent l-mer index query whose blocks (one per SM) take
+(SV tile, row) items from a device work queue, tile-major, then the per-row
+finish.  Replaying a graph costs one launch.
+
+Linear kernels with an l-mer table score through the table instead (a
+self-kernel plus W lookups per row), also captured.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import engine
+from .kernels import RbfKernel
+
+_ROW_GRANULE = 1024
+
+
+def _bucket_len(L: int) -> int:
+    b = 64
+    while b < L:
+        b *= 2
+    return b
+
+
+def _bucket_rows(B: int) -> int:
+    return max(_ROW_GRANULE, -(-B // _ROW_GRANULE) * _ROW_GRANULE)
+
+
+class _Graph:
+    def __init__(self, scorer, rows: int, L: int):
+        m = scorer.model
+        dev = m._device
+        self.rows, self.L = rows, L
+        self.codes = torch.zeros((rows, L), dtype=torch.uint8, device=dev)
+        self.lengths = torch.zeros(rows, dtype=torch.int64, device=dev)
+        self.out = torch.empty(rows, dtype=torch.float64, device=dev)
+        self.graph = None
+        self.scorer = scorer
+
+    def _prep(self):
+        s = self.scorer
+        spec = s.model._spec()
+        self.fwd, self.rc, self.counts = engine.pack(spec, self.codes, self.lengths)
+        if s.table is not None:
+            return
+        if s.normalize:
+            dx = engine.self_kernel(spec, self.fwd, self.rc, self.counts)
+            self.inv_dx = 1.0 / torch.sqrt(torch.clamp(dx, min=1e-20))
+        else:
+            self.inv_dx = torch.ones(self.rows, dtype=torch.float64, device=self.fwd.device)
+        self.order = torch.argsort(self.counts, descending=True).to(torch.int32)
+
+    def _query(self):
+        s = self.scorer
+        m = s.model
+        if s.table is not None:
+            self.out.copy_(engine.table_score(m._spec(), s.table, self.fwd, self.rc, self.counts, m.bias,
+                                              s.normalize))
+            return
+        s.index.score(self.fwd, self.counts, self.inv_dx, s.inv_ds, s.coef, s.gamma, s.rbf, m.bias, self.order,
+                      out=self.out, check=False)
+
+    def _body(self):
+        self._prep()
+        self._query()
+
+    def _capture(self):
+        # warm-up on a side stream, then capture the two phases (the work-queue
+        # counter, the stream-ordered scratch and every kernel go into them)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self._body()
+        torch.cuda.current_stream().wait_stream(side)
+        self.g_prep = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.g_prep):
+            self._prep()
+        self.g_query = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.g_query, pool=self.g_prep.pool()):
+            self._query()
+        self.graph = True
+
+    def run(self, events=None):
+        """Replay; events (start, end): recorded around the query phase."""
+        if self.graph is None:
+            self._capture()
+        self.g_prep.replay()
+        if events:
+            events[0].record()
+        self.g_query.replay()
+        if events:
+            events[1].record()
+
+
+class BatchedScorer:
+    """Scores [B, L] code batches against model's SVs in graph-captured
+    launches; results equal model(x) (same kernels, same order of sums)."""
+
+    def __init__(self, model, use_graphs: bool = True):
+        self.model = model
+        kernel = model.kernel
+        self.normalize = kernel.base.normalize
+        self.rbf = isinstance(kernel, RbfKernel)
+        self.gamma = kernel.gamma if self.rbf else 0.0
+        self.table = model._lmer_table_for()
+        self.index = None
+        if self.table is None:
+            self.index = model._sv_index()
+            if self.index is None:
+                raise ValueError("batched scoring needs the l-mer index or the l-mer table")
+            self.inv_ds = model._inv_ds()
+            self.coef = model._sv_coef()
+        self.use_graphs = use_graphs
+        self._graphs: dict = {}
+
+    def _graph(self, B: int, L: int) -> _Graph:
+        key = (_bucket_rows(B), _bucket_len(L))
+        g = self._graphs.get(key)
+        if g is None:
+            g = self._graphs[key] = _Graph(self, *key)
+        return g
+
+    def score(self, codes: torch.Tensor, lengths: torch.Tensor | None = None, events=None,
+              check: bool = True) -> torch.Tensor:
+        """[B] float64 scores (bias included) of device codes [B, L] with
+        device lengths [B] (None: every row L long).  events: optional CUDA
+        events recorded around the query phase.  check=False skips the index
+        flag read (no synchronisation); call check_flags() later."""
+        B, L = codes.shape
+        g = self._graph(B, L)
+        self._last = g
+        g.codes[:B, :L].copy_(codes)
+        if L < g.L:
+            g.codes[:B, L:].zero_()
+        if lengths is None:
+            g.lengths[:B].fill_(L)
+        else:
+            g.lengths[:B].copy_(lengths)
+        g.lengths[B:].zero_()
+        if self.use_graphs:
+            g.run(events)
+        else:
+            g._prep()
+            if events:
+                events[0].record()
+            g._query()
+            if events:
+                events[1].record()
+        if check:
+            self.check_flags(g)
+        return g.out[:B]
+
+    def check_flags(self, g=None):
+        """Reads the index flags (synchronises); reruns the last batch eagerly
+        with 32-bit counters when a block's 16-bit carries outgrew its log."""
+        if g is None:
+            g = self._last
+        if self.index is not None:
+            # (reads the index flags: synchronises the stream) a block whose
+            # 16-bit counters carried past its log reruns eagerly with 32-bit
+            # counters; the graph keeps the fast kernel
+            f = self.index.flags()
+            if f & 1:
+                self.index.set_wide(True)
+                try:
+                    g._body()
+                    f = self.index.flags()
+                finally:
+                    self.index.set_wide(False)
+            if f & 2:
+                from ._lib import GKM_ERR_CAPACITY, GkmError
+
+                raise GkmError(GKM_ERR_CAPACITY, "a weighted pair count passed 2^32")

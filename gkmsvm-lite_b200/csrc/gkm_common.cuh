@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/gkm_b200.h"
 
 #define GKM_FULL 0xFFFFFFFFu
@@ -116,7 +118,13 @@ struct gkm_index {
     int32_t acc_bytes;   // shared memory left for counters in a query block
     int32_t wide;        // 1: 32-bit counters (weighted, or after a carry-log overflow)
     int *status;         // device flags set by queries (see gkm_index_status)
+    unsigned int *queues;            // [GKM_QUEUE_SLOTS] work-queue heads, one per call in flight
+    mutable std::atomic<unsigned> next_queue{0};
 };
+
+// Concurrent query calls on one index (different streams) each take their own
+// work-queue counter; more than this many in flight at once would share one.
+#define GKM_QUEUE_SLOTS 64
 
 int gkm_smem_limit();
 int gkm_sm_count();

@@ -283,6 +283,9 @@ struct QueryArgs {
     const uint8_t *wd;
     const uint8_t *wq;    // [rows, W] query window weights (null: from the row's count)
     int *status;          // bit 0: a block's carry log overflowed; bit 1: a wide counter wrapped
+    unsigned int *queue;  // work-queue head: items (tile, row) handed out tile-major
+    int64_t B;            // rows
+    int tiles;
     // score
     const double *inv_dx;
     const double *inv_ds;
@@ -372,22 +375,32 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
     uint32_t *sm_masks = n_masks <= MASKS_SMEM_MAX ? (uint32_t *)smraw : nullptr;
     uint32_t *sm_log = (uint32_t *)(smraw + ((sm_masks ? (size_t)n_masks * 4 : 0) + 15 & ~(size_t)15));
     uint32_t *sm_acc = (uint32_t *)(smraw + query_fixed_smem(n_masks));
-    const int64_t r = blockIdx.x;
-    const int64_t row = a.order ? a.order[r] : r;
-    const int t = blockIdx.y;
-    const int St = a.tile_svs;
-    const int64_t s0 = (int64_t)t * St;
-    const int ns = (int)min((int64_t)St, a.S - s0);
-    const int64_t lo_g = a.diag_offset >= 0 ? a.diag_offset + row : 0;
-    if (MODE == MODE_RAW && s0 + ns <= lo_g) return;  // tile wholly below the diagonal
-    const uint32_t lo = (uint32_t)(lo_g > s0 ? lo_g - s0 : 0);
+    __shared__ unsigned int item_s;
     if (sm_masks)
         for (int k = threadIdx.x; k < n_masks; k += Q_THREADS) sm_masks[k] = a.masks[k];
     const uint32_t *masks = sm_masks ? sm_masks : a.masks;
+    const int St = a.tile_svs;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // persistent: each block takes (tile, row) items off the work queue,
+    // tile-major so that one SV tile's index stays in L2, rows in the order
+    // given (longest first)
+    for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) item_s = atomicAdd(a.queue, 1u);
+    __syncthreads();
+    const unsigned int item = item_s;
+    if ((int64_t)item >= a.B * a.tiles) break;
+    const int t = (int)(item / a.B);
+    const int64_t r = item - (int64_t)t * a.B;
+    const int64_t row = a.order ? a.order[r] : r;
+    const int64_t s0 = (int64_t)t * St;
+    const int ns = (int)min((int64_t)St, a.S - s0);
+    const int64_t lo_g = a.diag_offset >= 0 ? a.diag_offset + row : 0;
+    if (MODE == MODE_RAW && s0 + ns <= lo_g) continue;  // tile wholly below the diagonal
+    const uint32_t lo = (uint32_t)(lo_g > s0 ? lo_g - s0 : 0);
     const int n = a.cx[row];
     const uint32_t *x = a.bx + row * a.W;
     const uint32_t *off = a.off + (int64_t)t * a.n_lmers;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double inv_dx = MODE == MODE_SCORE ? a.inv_dx[row] : 0.0;
     double part = 0.0;
     const int sub = C16 ? ns : a.sub_svs;
@@ -486,7 +499,8 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
     }
     if (MODE == MODE_SCORE) {
         part = gkm_block_sum(part, red);
-        if (threadIdx.x == 0) a.partial[row * gridDim.y + t] = part;
+        if (threadIdx.x == 0) a.partial[row * a.tiles + t] = part;
+    }
     }
 }
 
@@ -621,7 +635,8 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
         eb = sizeof(uint32_t) * ((size_t)total + 8);
         if ((compact ? cudaMalloc(&ix->ent16, eb16) : cudaMalloc(&ix->ent, eb)) != cudaSuccess ||
             cudaMalloc(&ix->masks, sizeof(uint32_t) * n_masks) != cudaSuccess ||
-            cudaMalloc(&ix->status, sizeof(int)) != cudaSuccess) {
+            cudaMalloc(&ix->status, sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&ix->queues, sizeof(unsigned int) * GKM_QUEUE_SLOTS) != cudaSuccess) {
             status = gkm_fail(GKM_ERR_OOM, "index entries");
             break;
         }
@@ -663,6 +678,7 @@ extern "C" int gkm_index_free(gkm_index_t *ix)
     cudaFree(ix->ent16);
     cudaFree(ix->masks);
     cudaFree(ix->status);
+    cudaFree(ix->queues);
     delete ix;
     return GKM_OK;
 }
@@ -719,7 +735,7 @@ static QueryArgs query_args(const gkm_index_t *ix, const uint32_t *bx, const int
 }
 
 template <bool WEIGHTED, int MODE, bool C16, bool E16>
-static void launch_query(dim3 grid, size_t smem, cudaStream_t st, const QueryArgs &a)
+static void launch_query(unsigned grid, size_t smem, cudaStream_t st, const QueryArgs &a)
 {
     // ids need a range test only for a self-Gram's diagonal or wide sub-ranges
     if (C16 && a.diag_offset < 0) {
@@ -736,19 +752,30 @@ static void launch_query(dim3 grid, size_t smem, cudaStream_t st, const QueryArg
 template <int MODE>
 static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cudaStream_t st)
 {
-    if (B > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many rows for one launch");
+    if (B * ix->tiles > 0xFFFFFFFFLL - 2LL * gkm_sm_count())
+        return gkm_fail(GKM_ERR_UNSUPPORTED, "too many (row, tile) items for one launch");
     size_t smem = query_fixed_smem(ix->n_masks) + 16 + (size_t)ix->acc_bytes;
-    dim3 grid((unsigned)B, (unsigned)ix->tiles);
+    // one resident block per SM, fed by the work queue (a counter of the
+    // index's pool, one per call in flight)
+    QueryArgs q = a;
+    q.B = B;
+    q.tiles = ix->tiles;
+    unsigned slot = ix->next_queue.fetch_add(1) % GKM_QUEUE_SLOTS;
+    q.queue = ix->queues + slot;
+    cudaError_t e0 = cudaMemsetAsync(q.queue, 0, sizeof(unsigned int), st);
+    if (e0 != cudaSuccess) return gkm_cuda_status(e0, "index queue");
+    int64_t items = B * ix->tiles;
+    unsigned grid = (unsigned)(items < gkm_sm_count() ? items : gkm_sm_count());
     if (ix->spec.weighted)
-        launch_query<true, MODE, false, false>(grid, smem, st, a);
+        launch_query<true, MODE, false, false>(grid, smem, st, q);
     else if (ix->ent16 && ix->wide)
-        launch_query<false, MODE, false, true>(grid, smem, st, a);
+        launch_query<false, MODE, false, true>(grid, smem, st, q);
     else if (ix->ent16)
-        launch_query<false, MODE, true, true>(grid, smem, st, a);
+        launch_query<false, MODE, true, true>(grid, smem, st, q);
     else if (ix->wide)
-        launch_query<false, MODE, false, false>(grid, smem, st, a);
+        launch_query<false, MODE, false, false>(grid, smem, st, q);
     else
-        launch_query<false, MODE, true, false>(grid, smem, st, a);
+        launch_query<false, MODE, true, false>(grid, smem, st, q);
     GKM_CHECK_LAUNCH("index_query");
     return GKM_OK;
 }

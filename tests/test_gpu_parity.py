@@ -344,3 +344,34 @@ def test_counter_carries_are_exact():
     got = _np(m(x))
     want = orc.scores(orc.OracleModel(sv, None, coef, 0.0, kd), x)
     np.testing.assert_allclose(got, want, rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.parametrize("name", ["t2", "t3", "t4", "t5", "t6", "t0"])
+@pytest.mark.parametrize("graphs", [True, False])
+def test_batched_scorer_equals_model(small, name, graphs):
+    """Graph-captured batched scoring gives model(x)'s scores (short rows are
+    masked by the caller, as model(x) does)."""
+    from gkmsvm_lite_b200.batch import BatchedScorer
+
+    c = small[name]
+    m = _model(c, use_lmer_table=False)
+    x, xl = c["x"][:-1], c["x_lengths"][:-1]
+    bs = BatchedScorer(m, use_graphs=graphs)
+    for _ in range(2):  # capture, then replay
+        got = _np(bs.score(torch.from_numpy(x).cuda(), torch.from_numpy(xl).cuda()))
+        np.testing.assert_allclose(got, c["scores"][:-1, 0], rtol=RTOL, atol=ATOL)
+
+
+def test_batched_scorer_config1_table_and_index():
+    import gkmsvm_lite_b200.synthetic as syn
+    from gkmsvm_lite_b200.batch import BatchedScorer
+
+    w = syn.config1()
+    want = np.load(os.path.join(GOLDEN, "config1.npz"))["scores"][:, 0]
+    for table in (False, True):
+        m = gk.GkmSVM(w.sv, w.coef, 0.0, "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}).cuda()
+        m.use_lmer_table = table
+        bs = BatchedScorer(m)
+        x = torch.from_numpy(w.x).cuda()
+        for _ in range(2):
+            np.testing.assert_allclose(_np(bs.score(x)), want, rtol=RTOL, atol=ATOL)
