@@ -81,11 +81,13 @@ class _Graph:
         with torch.cuda.stream(side):
             self._body()
         torch.cuda.current_stream().wait_stream(side)
+        # thread-local capture: other threads (a server's side stream) may keep
+        # issuing CUDA work meanwhile
         self.g_prep = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.g_prep):
+        with torch.cuda.graph(self.g_prep, capture_error_mode="thread_local"):
             self._prep()
         self.g_query = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.g_query, pool=self.g_prep.pool()):
+        with torch.cuda.graph(self.g_query, pool=self.g_prep.pool(), capture_error_mode="thread_local"):
             self._query()
         self.graph = True
 
@@ -138,6 +140,8 @@ class BatchedScorer:
         B, L = codes.shape
         g = self._graph(B, L)
         self._last = g
+        if self.index is not None:
+            self._before = self.index.counters()
         g.codes[:B, :L].copy_(codes)
         if L < g.L:
             g.codes[:B, L:].zero_()
@@ -160,23 +164,10 @@ class BatchedScorer:
         return g.out[:B]
 
     def check_flags(self, g=None):
-        """Reads the index flags (synchronises); reruns the last batch eagerly
-        with 32-bit counters when a block's 16-bit carries outgrew its log."""
+        """Waits for the last batch; reruns it eagerly with 32-bit counters if
+        a query block's 16-bit carries outgrew its log meanwhile (the graph
+        keeps the fast kernel)."""
         if g is None:
             g = self._last
         if self.index is not None:
-            # (reads the index flags: synchronises the stream) a block whose
-            # 16-bit counters carried past its log reruns eagerly with 32-bit
-            # counters; the graph keeps the fast kernel
-            f = self.index.flags()
-            if f & 1:
-                self.index.set_wide(True)
-                try:
-                    g._body()
-                    f = self.index.flags()
-                finally:
-                    self.index.set_wide(False)
-            if f & 2:
-                from ._lib import GKM_ERR_CAPACITY, GkmError
-
-                raise GkmError(GKM_ERR_CAPACITY, "a weighted pair count passed 2^32")
+            self.index.settle(self._before, g._body)

@@ -282,7 +282,7 @@ struct QueryArgs {
     double h[16];
     const uint8_t *wd;
     const uint8_t *wq;    // [rows, W] query window weights (null: from the row's count)
-    int *status;          // bit 0: a block's carry log overflowed; bit 1: a wide counter wrapped
+    unsigned int *status; // [2] event counts: a block's carry log overflowed, a wide counter wrapped
     unsigned int *queue;  // work-queue head: items (tile, row) handed out tile-major
     int64_t B;            // rows
     int tiles;
@@ -333,7 +333,7 @@ __device__ __forceinline__ int64_t read_count(const uint32_t *acc, const uint32_
 
 // C16 counter update: add (1 << 16 * half) to word; fmask selects the field.
 __device__ __forceinline__ void count16(uint32_t *acc, uint32_t word, uint32_t add, uint32_t fmask, int *nlog,
-                                        uint32_t *log, int *status)
+                                        uint32_t *log, unsigned int *status)
 {
     const uint32_t old = atomicAdd(acc + word, add);
     if ((old & fmask) == fmask) {  // the field was 0xFFFF: it carries
@@ -347,7 +347,7 @@ __device__ __forceinline__ void count16(uint32_t *acc, uint32_t word, uint32_t a
                 if (old == 0xFFFFFFFFu) log[p0 + 1] = (word << 1) | EV_WRAP;
             }
         } else {
-            atomicOr(status, 1);
+            atomicAdd(status, 1u);
         }
     }
 }
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                         else {
                             const uint32_t inc = WEIGHTED ? wq * (en[q] >> 24) : 1u;
                             const uint32_t old = atomicAdd(sm_acc + base + id, inc);
-                            if (old + inc < old) atomicOr(a.status, 2);
+                            if (old + inc < old) atomicAdd(a.status + 1, 1u);
                         }
                     }
                 }
@@ -635,7 +635,7 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
         eb = sizeof(uint32_t) * ((size_t)total + 8);
         if ((compact ? cudaMalloc(&ix->ent16, eb16) : cudaMalloc(&ix->ent, eb)) != cudaSuccess ||
             cudaMalloc(&ix->masks, sizeof(uint32_t) * n_masks) != cudaSuccess ||
-            cudaMalloc(&ix->status, sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&ix->status, 2 * sizeof(unsigned int)) != cudaSuccess ||
             cudaMalloc(&ix->queues, sizeof(unsigned int) * GKM_QUEUE_SLOTS) != cudaSuccess) {
             status = gkm_fail(GKM_ERR_OOM, "index entries");
             break;
@@ -650,7 +650,7 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
             cudaMemcpyAsync(ix->ent, vals, sizeof(uint32_t) * (size_t)total, cudaMemcpyDeviceToDevice, st);
         }
         cudaMemcpyAsync(ix->masks, masks, sizeof(uint32_t) * n_masks, cudaMemcpyDeviceToDevice, st);
-        cudaMemsetAsync(ix->status, 0, sizeof(int), st);
+        cudaMemsetAsync(ix->status, 0, 2 * sizeof(unsigned int), st);
         ix->bytes = (int64_t)sizeof(uint32_t) * (nbuckets + 1) + (int64_t)eb + sizeof(uint32_t) * n_masks;
     } while (0);
     cudaFreeAsync(ecount, st);
@@ -683,17 +683,13 @@ extern "C" int gkm_index_free(gkm_index_t *ix)
     return GKM_OK;
 }
 
-extern "C" int gkm_index_status(gkm_index_t *ix, int32_t *flags, int32_t wide, gkm_stream_t stream)
+extern "C" int gkm_index_status(gkm_index_t *ix, uint32_t *counts, int32_t wide, gkm_stream_t stream)
 {
     if (!ix) return gkm_fail(GKM_ERR_INVALID, "null index");
-    cudaStream_t st = (cudaStream_t)stream;
-    if (flags) {
-        int v = 0;
-        cudaError_t e = cudaMemcpyAsync(&v, ix->status, sizeof(int), cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (counts) {
+        cudaError_t e = cudaMemcpyAsync(counts, ix->status, 2 * sizeof(unsigned int), cudaMemcpyDefault,
+                                        (cudaStream_t)stream);
         if (e != cudaSuccess) return gkm_cuda_status(e, "index status");
-        *flags = v;
-        if (v) cudaMemsetAsync(ix->status, 0, sizeof(int), st);
     }
     if (wide >= 0) ix->wide = ix->spec.weighted ? 1 : wide;
     return GKM_OK;

@@ -119,30 +119,41 @@ class DeviceIndex:
         except Exception:
             pass
 
-    def flags(self) -> int:
-        """Query flags since the last read (synchronises the stream)."""
-        f = ctypes.c_int32()
-        call("gkm_index_status", self.handle, ctypes.byref(f), -1, _st())
-        return f.value
+    def counters(self) -> torch.Tensor:
+        """A pinned host snapshot of the index's event counts, copied in
+        stream order (read it after the stream reaches this point)."""
+        buf = torch.empty(2, dtype=torch.int32, pin_memory=True)
+        call("gkm_index_status", self.handle, ptr(buf), -1, _st())
+        return buf
 
     def set_wide(self, wide: bool) -> None:
         call("gkm_index_status", self.handle, None, int(bool(wide)), _st())
 
-    def checked(self, run):
-        """run() through the index; when a query block's 16-bit counters
-        carried more often than its log holds, run it again with 32-bit
-        counters (exact either way); a wrapped 32-bit counter raises."""
-        out = run()
-        f = self.flags()
-        if f & 1:
+    def settle(self, before: torch.Tensor, rerun=None):
+        """After a call bracketed by counters() snapshots: waits for the
+        stream; if a query block's 16-bit carries outgrew its log anywhere in
+        that window (this call's or a concurrent one's), reruns rerun() with
+        32-bit counters (exact either way).  A wrapped 32-bit count raises."""
+        after = self.counters()
+        torch.cuda.current_stream().synchronize()
+        if int(after[0]) != int(before[0]) and rerun is not None:
             self.set_wide(True)
             try:
-                out = run()
-                f = self.flags()
+                b2 = self.counters()
+                rerun()
+                after = self.counters()
+                torch.cuda.current_stream().synchronize()
+                before = b2
             finally:
                 self.set_wide(False)
-        if f & 2:
+        if int(after[1]) != int(before[1]):
             raise _lib.GkmError(_lib.GKM_ERR_CAPACITY, "a weighted pair count passed 2^32 for one (row, SV) pair")
+
+    def checked(self, run):
+        """run() through the index, exact: see settle()."""
+        before = self.counters()
+        out = run()
+        self.settle(before, run)
         return out
 
     def pairwise(self, bx, cx, diag_offset=None, raw=True, profile=False, out=None):

@@ -1,0 +1,330 @@
+"""Serving: a device-resident request loop with continuous batching.
+
+GkmServer keeps one model's SV index in HBM and takes mixed requests --
+predict, score_variants, ism, gkmexplain -- from any thread (submit returns a
+Future).  A scheduler thread admits waiting requests into the next scoring
+batch as long as the batch's row budget and the device's free memory allow
+(requests that do not fit wait; a request larger than the whole budget is
+refused), merges every predict and variant row of the batch into one
+graph-captured scoring pass, and keeps up to two such passes in flight on
+separate streams, so requests that arrive while a batch runs are admitted as
+soon as a slot frees up.  ISM and GkmExplain requests run on their own worker
+stream beside the scoring passes.  Every request's latency (submit to result)
+is recorded; stats() gives p50/p99 per request type and sequences per second.
+
+The scheduling is independent of the device work: a backend object runs the
+batches (GpuBackend here; the tests drive the same loop with a host fake).
+"""
+
+from __future__ import annotations
+
+import queue
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+
+import numpy as np
+
+KINDS = ("predict", "score_variants", "ism", "explain")
+
+
+class AdmissionError(RuntimeError):
+    """The request can never be admitted (larger than the budget) or is malformed."""
+
+
+@dataclass
+class Request:
+    kind: str
+    x: object = None                # predict/ism/explain: codes [n, L] or list of strings
+    lengths: object = None
+    alt: object = None              # score_variants: alt alleles
+    alt_lengths: object = None
+    mode: str = "hypothetical"      # explain mode
+    future: Future = field(default_factory=Future)
+    t_submit: float = 0.0
+    rows: int = 0                   # scoring rows it adds to a batch
+    bytes: int = 0                  # device memory it needs while it runs
+    t_start: float = 0.0
+
+
+def _percentiles(v):
+    if not v:
+        return {"n": 0}
+    a = np.asarray(v) * 1e3
+    return {"n": len(a), "p50_ms": float(np.percentile(a, 50)), "p99_ms": float(np.percentile(a, 99)),
+            "mean_ms": float(a.mean())}
+
+
+class GkmServer:
+    """Continuous-batching request loop over one model (see the module doc)."""
+
+    def __init__(self, backend, *, max_batch_rows: int = 8192, max_inflight: int = 2,
+                 memory_reserve: int = 2 << 30, max_wait_s: float = 0.002):
+        self.backend = backend
+        self.max_batch_rows = max_batch_rows
+        self.max_inflight = max_inflight
+        self.memory_reserve = memory_reserve
+        self.max_wait_s = max_wait_s
+        self._in: queue.Queue = queue.Queue()
+        self._side: queue.Queue = queue.Queue()
+        self._waiting: list[Request] = []
+        self._inflight: list = []  # (handle, [requests])
+        self._lat: dict = {k: [] for k in KINDS}
+        self._seqs = 0
+        self._t0 = None
+        self._stop = threading.Event()
+        self._threads: list[threading.Thread] = []
+        self._lock = threading.Lock()
+        self.admitted = 0
+        self.deferred = 0
+        self.rejected = 0
+
+    # -- client side ---------------------------------------------------------
+
+    def submit(self, kind: str, x=None, *, lengths=None, alt=None, alt_lengths=None, mode="hypothetical") -> Future:
+        if kind not in KINDS:
+            raise ValueError(f"kind must be one of {KINDS}, got {kind!r}")
+        r = Request(kind, x, lengths, alt, alt_lengths, mode)
+        r.t_submit = time.perf_counter()
+        try:
+            self.backend.prepare(r)
+        except Exception as e:  # malformed request: fail it, never the loop
+            self.rejected += 1
+            r.future.set_exception(e)
+            return r.future
+        if r.kind in ("predict", "score_variants") and r.rows > self.max_batch_rows:
+            self.rejected += 1
+            r.future.set_exception(AdmissionError(
+                f"{r.rows} rows exceed the batch budget of {self.max_batch_rows}; split the request"))
+            return r.future
+        (self._in if r.kind in ("predict", "score_variants") else self._side).put(r)
+        return r.future
+
+    # -- loop ------------------------------------------------------------------
+
+    def start(self):
+        self._t0 = time.perf_counter()
+        self._stop.clear()
+        self._threads = [threading.Thread(target=self._score_loop, daemon=True),
+                         threading.Thread(target=self._side_loop, daemon=True)]
+        for t in self._threads:
+            t.start()
+        return self
+
+    def stop(self, timeout: float = 60.0):
+        self._stop.set()
+        for t in self._threads:
+            t.join(timeout)
+        self._threads = []
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *a):
+        self.stop()
+
+    def _free_memory(self) -> int:
+        return self.backend.free_memory() - self.memory_reserve
+
+    def _score_loop(self):
+        while not (self._stop.is_set() and not self._waiting and not self._inflight and self._in.empty()):
+            # take everything that has arrived
+            try:
+                timeout = 0.0005 if (self._waiting or self._inflight) else 0.01
+                self._waiting.append(self._in.get(timeout=timeout))
+                while True:
+                    self._waiting.append(self._in.get_nowait())
+            except queue.Empty:
+                pass
+            # retire finished batches first: that frees slots and memory
+            still = []
+            for handle, reqs in self._inflight:
+                if self.backend.done(handle):
+                    self._finish_batch(handle, reqs)
+                else:
+                    still.append((handle, reqs))
+            self._inflight = still
+            if not self._waiting or len(self._inflight) >= self.max_inflight:
+                continue
+            # admit in arrival order while the row budget and free memory allow
+            batch, rows, need = [], 0, 0
+            free = self._free_memory()
+            for r in list(self._waiting):
+                if rows + r.rows > self.max_batch_rows or need + r.bytes > free:
+                    self.deferred += 1
+                    break
+                batch.append(r)
+                rows += r.rows
+                need += r.bytes
+            if not batch:
+                if not self._inflight and self._waiting and self._waiting[0].bytes > free:
+                    r = self._waiting.pop(0)  # can never fit: refuse it
+                    self.rejected += 1
+                    r.future.set_exception(AdmissionError("not enough free device memory for this request"))
+                continue
+            for r in batch:
+                self._waiting.remove(r)
+                r.t_start = time.perf_counter()
+            self.admitted += len(batch)
+            try:
+                handle = self.backend.launch_scoring(batch)
+            except Exception as e:
+                for r in batch:
+                    r.future.set_exception(e)
+                continue
+            self._inflight.append((handle, batch))
+
+    def _finish_batch(self, handle, reqs):
+        try:
+            results = self.backend.collect_scoring(handle, reqs)
+        except Exception as e:
+            for r in reqs:
+                r.future.set_exception(e)
+            return
+        now = time.perf_counter()
+        with self._lock:
+            for r, res in zip(reqs, results):
+                self._lat[r.kind].append(now - r.t_submit)
+                self._seqs += r.rows
+                r.future.set_result(res)
+
+    def _side_loop(self):
+        while not (self._stop.is_set() and self._side.empty()):
+            try:
+                r = self._side.get(timeout=0.01)
+            except queue.Empty:
+                continue
+            while r.bytes > self._free_memory():
+                if self._stop.is_set():
+                    break
+                time.sleep(0.001)
+            r.t_start = time.perf_counter()
+            try:
+                res = self.backend.run_side(r)
+            except Exception as e:
+                r.future.set_exception(e)
+                continue
+            now = time.perf_counter()
+            with self._lock:
+                self._lat[r.kind].append(now - r.t_submit)
+                self._seqs += r.rows
+            r.future.set_result(res)
+
+    def stats(self) -> dict:
+        with self._lock:
+            wall = time.perf_counter() - (self._t0 or time.perf_counter())
+            out = {k: _percentiles(v) for k, v in self._lat.items()}
+            allv = [x for v in self._lat.values() for x in v]
+            out["all"] = _percentiles(allv)
+            out["seqs_per_sec"] = self._seqs / wall if wall > 0 else 0.0
+            out["admitted"], out["deferred"], out["rejected"] = self.admitted, self.deferred, self.rejected
+            return out
+
+
+class GpuBackend:
+    """Runs a GkmServer's batches on the model's GPU: scoring rows through
+    BatchedScorer (two instances, one per in-flight slot, each on its own
+    stream), ISM and GkmExplain through the model's own calls on a side stream."""
+
+    def __init__(self, model, slots: int = 2):
+        import torch
+
+        from .batch import BatchedScorer
+
+        self.model = model
+        self.torch = torch
+        model._sv_index()
+        model._sv_diag()
+        self.scorers = [BatchedScorer(model) for _ in range(slots)]
+        self.streams = [torch.cuda.Stream() for _ in range(slots)]
+        self.side_stream = torch.cuda.Stream()
+        self._slot = 0
+        self._busy = [False] * slots
+
+    def free_memory(self) -> int:
+        free, _ = self.torch.cuda.mem_get_info()
+        return int(free)
+
+    def prepare(self, r: Request):
+        from .inputs import allele_arrays, as_batch
+
+        if r.kind == "score_variants":
+            ref, alt, rl, al = allele_arrays(r.x, r.alt, r.lengths, r.alt_lengths)
+            r.x, r.alt, r.lengths, r.alt_lengths = ref, alt, rl, al
+            n, L = ref.shape
+            r.rows = 2 * n
+        else:
+            x, ln = as_batch(r.x, r.lengths)
+            r.x, r.lengths = x, ln
+            n, L = x.shape
+            r.rows = n
+        # packed windows + scratch of its rows (ISM: mutant window sets too)
+        r.bytes = r.rows * L * 16 + (L * 4 * 5 * 8 * self.model.num_support_vectors if r.kind == "ism" else 0)
+
+    def launch_scoring(self, batch):
+        torch = self.torch
+        slot = self._busy.index(False)
+        self._busy[slot] = True
+        rows, lens, spans = [], [], []
+        L = 0
+        for r in batch:
+            if r.kind == "predict":
+                parts = [(r.x, r.lengths)]
+            else:
+                parts = [(r.alt, r.alt_lengths), (r.x, r.lengths)]
+            start = len(rows)
+            for x, ln in parts:
+                x = np.asarray(x)
+                L = max(L, x.shape[1])
+                for i in range(x.shape[0]):
+                    rows.append(x[i])
+                    lens.append(x.shape[1] if ln is None else int(ln[i]))
+            spans.append((start, len(rows)))
+        codes = np.zeros((len(rows), L), np.uint8)
+        for i, x in enumerate(rows):
+            codes[i, : len(x)] = x
+        lens = np.asarray(lens, np.int64)
+        stream = self.streams[slot]
+        with torch.cuda.stream(stream):
+            xd = torch.from_numpy(codes).pin_memory().to(self.model._device, non_blocking=True)
+            ld = torch.from_numpy(lens).pin_memory().to(self.model._device, non_blocking=True)
+            out = self.scorers[slot].score(xd, ld, check=False)
+            host = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
+            host.copy_(out, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record()
+        return (slot, ev, host, spans, lens)
+
+    def done(self, handle) -> bool:
+        return handle[1].query()
+
+    def collect_scoring(self, handle, reqs):
+        slot, ev, host, spans, lens = handle
+        ev.synchronize()
+        with self.torch.cuda.stream(self.streams[slot]):
+            self.scorers[slot].check_flags()
+        self._busy[slot] = False
+        scores = host.numpy().copy()
+        l = self.model.kernel.l
+        scores[lens < l] = np.nan
+        out = []
+        for r, (a, b) in zip(reqs, spans):
+            s = scores[a:b, None]
+            if r.kind == "score_variants":
+                n = (b - a) // 2
+                s = s[:n] - s[n:]
+            out.append(s)
+        return out
+
+    def run_side(self, r: Request):
+        from .explain import gkmexplain
+        from .ism import ism
+
+        torch = self.torch
+        with torch.cuda.stream(self.side_stream):
+            if r.kind == "ism":
+                res = ism(self.model, r.x, lengths=r.lengths)
+            else:
+                res = gkmexplain(self.model, r.x, lengths=r.lengths, mode=r.mode)
+            return res.cpu().numpy()

@@ -92,12 +92,14 @@ int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const uint32_t *
 int gkm_index_free(gkm_index_t *index);
 int gkm_index_info(const gkm_index_t *index, int64_t *entries, int32_t *tiles,
                    int32_t *tile_svs, int64_t *device_bytes);
-/* Reads (synchronising the stream) and clears the index's query flags into
- * *flags (nullable): bit 0 = a query block's 16-bit counter carries
- * overflowed its log, bit 1 = a 32-bit counter wrapped; queries since the
- * last read that set a flag must be rerun.  wide >= 0 selects 32-bit counters
- * (1) or 16-bit counters with the carry log (0) for unweighted kernels. */
-int gkm_index_status(gkm_index_t *index, int32_t *flags, int32_t wide, gkm_stream_t stream);
+/* Copies, in stream order (cudaMemcpyAsync), the index's two event counts
+ * into counts[2] (nullable; host or device memory): [0] query blocks whose
+ * 16-bit counter carries outgrew their log, [1] 32-bit counters that wrapped.
+ * The counts only grow: a call whose window (copy before, copy after, on its
+ * stream) sees [0] change reruns with 32-bit counters; [1] changing is an
+ * error.  wide >= 0 selects 32-bit counters (1) or 16-bit counters with the
+ * carry log (0) for unweighted kernels. */
+int gkm_index_status(gkm_index_t *index, uint32_t *counts, int32_t wide, gkm_stream_t stream);
 
 /* K_raw [B, S] (nullable) and profiles [B, S, l+1] (nullable) through the
  * index; diag_offset >= 0: row b is column diag_offset + b of a self-Gram and

@@ -1,0 +1,98 @@
+"""The serving loop's scheduling on the host, with a fake backend: continuous
+batching (requests arriving during a batch join the next one while it is still
+in flight), admission by free device memory, refusal of requests that can
+never fit, malformed requests failing alone, and latency statistics.  No GPU."""
+
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from gkmsvm_lite_b200.serve import AdmissionError, GkmServer
+
+
+class FakeBackend:
+    def __init__(self, free=1 << 40, delay=0.02):
+        self.free = free
+        self.delay = delay
+        self.batches = []
+        self.inflight = 0
+        self.max_inflight_seen = 0
+        self.lock = threading.Lock()
+
+    def free_memory(self):
+        return self.free
+
+    def prepare(self, r):
+        if r.x is None:
+            raise ValueError("no sequences")
+        x = np.asarray(r.x)
+        r.rows = x.shape[0] * (2 if r.kind == "score_variants" else 1)
+        r.bytes = r.rows * 1000
+
+    def launch_scoring(self, batch):
+        with self.lock:
+            self.inflight += 1
+            self.max_inflight_seen = max(self.max_inflight_seen, self.inflight)
+            self.batches.append([id(r) for r in batch])
+        return (time.perf_counter() + self.delay, batch)
+
+    def done(self, h):
+        return time.perf_counter() >= h[0]
+
+    def collect_scoring(self, h, reqs):
+        with self.lock:
+            self.inflight -= 1
+        return [np.asarray(r.x).sum(axis=1, keepdims=True).astype(float) for r in reqs]
+
+    def run_side(self, r):
+        time.sleep(self.delay)
+        return np.asarray(r.x) * 2.0
+
+
+def test_results_and_continuous_batching():
+    be = FakeBackend(delay=0.05)
+    with GkmServer(be, max_batch_rows=64, max_inflight=2, memory_reserve=0) as srv:
+        futs = []
+        for i in range(40):
+            x = np.full((3, 5), i)
+            futs.append((i, srv.submit("predict", x)))
+            time.sleep(0.004)
+        side = srv.submit("ism", np.ones((1, 4)))
+        for i, f in futs:
+            np.testing.assert_array_equal(f.result(10), np.full((3, 1), 5 * i))
+        np.testing.assert_array_equal(side.result(10), np.full((1, 4), 2.0))
+        st = srv.stats()
+    assert len(be.batches) > 1 and max(len(b) for b in be.batches) > 1  # merged into batches
+    assert be.max_inflight_seen == 2  # a second batch started while the first ran
+    assert st["predict"]["n"] == 40 and st["predict"]["p99_ms"] >= st["predict"]["p50_ms"] > 0
+    assert st["ism"]["n"] == 1 and st["seqs_per_sec"] > 0
+
+
+def test_admission_waits_for_memory_and_refuses_what_never_fits():
+    be = FakeBackend(free=10_000, delay=0.02)
+    with GkmServer(be, max_batch_rows=1000, memory_reserve=0) as srv:
+        small = [srv.submit("predict", np.zeros((4, 3))) for _ in range(6)]  # 4,000 B each
+        huge = srv.submit("predict", np.zeros((20, 3)))  # 20,000 B > all free memory
+        for f in small:
+            assert f.result(10).shape == (4, 1)
+        with pytest.raises(AdmissionError):
+            huge.result(10)
+        st = srv.stats()
+    assert st["deferred"] > 0 and st["rejected"] == 1
+
+
+def test_bad_requests_fail_alone():
+    be = FakeBackend()
+    with GkmServer(be, max_batch_rows=8, memory_reserve=0) as srv:
+        with pytest.raises(ValueError):
+            srv.submit("nope", np.zeros((1, 3)))
+        bad = srv.submit("predict", None)
+        too_big = srv.submit("predict", np.zeros((9, 3)))
+        ok = srv.submit("predict", np.ones((2, 3)))
+        with pytest.raises(ValueError):
+            bad.result(5)
+        with pytest.raises(AdmissionError):
+            too_big.result(5)
+        np.testing.assert_array_equal(ok.result(5), [[3.0], [3.0]])
