@@ -187,6 +187,119 @@ def _sv_diag_threaded(sv, svl, kd):
         return np.concatenate(list(ex.map(one, parts)))
 
 
+def serving_leg(sv, svl, coef, n_requests=600, seed=4):
+    """Config 5: the 72k-SV t=5 (wgkmrbf, gamma=1) model served with continuous
+    batching.  Mixed requests (60% predict, 25% score-variants, 10% ISM, 5%
+    GkmExplain), lengths log-uniform 20..2000 bp, alt = one SNV (80%) or an
+    indel of 1..10 bp.  First all requests at once (capacity), then Poisson
+    arrivals at 70% of that rate for p50/p99 latency; beside it the plain
+    per-call form (each request its own call, one after another)."""
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+    import gkmsvm_lite_b200.synthetic as syn
+    from gkmsvm_lite_b200.serve import GkmServer, GpuBackend
+
+    rng = np.random.default_rng(seed)
+    model = gk.GkmSVM(sv, coef, 0.0, "wgkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 1.0}, sv_lengths=svl).cuda()
+    kinds = rng.choice(["predict", "score_variants", "ism", "explain"], size=n_requests, p=[0.6, 0.25, 0.1, 0.05])
+    reqs = []
+    for kind in kinds:
+        ln = syn.log_uniform_lengths(rng, 1, 20, 2000)
+        ln[0] = max(int(ln[0]), 11)
+        x = syn.ragged_codes(rng, ln)
+        r = {"kind": str(kind), "x": x, "lengths": ln}
+        if kind == "score_variants":
+            r["alt"], r["alt_lengths"] = syn.variant_pairs(rng, x, ln)
+        reqs.append(r)
+    backend = GpuBackend(model)
+
+    def submit_all(srv, rate=None):
+        futs = []
+        t0 = time.perf_counter()
+        gaps = rng.exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
+        t = t0
+        for r, g in zip(reqs, gaps):
+            t += g
+            d = t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            futs.append(srv.submit(r["kind"], r["x"], lengths=r["lengths"], alt=r.get("alt"),
+                                   alt_lengths=r.get("alt_lengths")))
+        for f in futs:
+            f.result(600)
+        return time.perf_counter() - t0
+
+    warm = GkmServer(backend).start()
+    for r in reqs[:24]:
+        warm.submit(r["kind"], r["x"], lengths=r["lengths"], alt=r.get("alt"), alt_lengths=r.get("alt_lengths")).result(600)
+    warm.stop()
+    srv = GkmServer(backend).start()
+    t_closed = submit_all(srv)
+    cap = srv.stats()
+    srv.stop()
+    rate = 0.7 * len(reqs) / t_closed
+    srv = GkmServer(backend).start()
+    submit_all(srv, rate)
+    open_stats = srv.stats()
+    srv.stop()
+    # plain per-call form: each request its own call, in order
+    t0 = time.perf_counter()
+    seqs = 0
+    for r in reqs:
+        if r["kind"] == "predict":
+            model(r["x"], lengths=r["lengths"]).cpu()
+            seqs += 1
+        elif r["kind"] == "score_variants":
+            model.score_variants(r["x"], r["alt"], ref_lengths=r["lengths"], alt_lengths=r["alt_lengths"]).cpu()
+            seqs += 2
+        elif r["kind"] == "ism":
+            gk.ism(model, r["x"], lengths=r["lengths"]).cpu()
+            seqs += 1
+        else:
+            gk.gkmexplain(model, r["x"], lengths=r["lengths"], mode="hypothetical").cpu()
+            seqs += 1
+    torch.cuda.synchronize()
+    plain = seqs / (time.perf_counter() - t0)
+    return {
+        "workload": "config5: 72,000 SVs t=5 wgkmrbf gamma=1; 60/25/10/5% predict/variants/ISM/explain, "
+                    f"{len(reqs)} requests, 20-2000 bp",
+        "capacity_seqs_per_sec": cap["seqs_per_sec"], "capacity_requests_per_sec": len(reqs) / t_closed,
+        "poisson_rate_requests_per_sec": rate,
+        "p50_ms": open_stats["all"].get("p50_ms"), "p99_ms": open_stats["all"].get("p99_ms"),
+        "by_kind_ms": {k: open_stats[k] for k in ("predict", "score_variants", "ism", "explain")},
+        "served_seqs_per_sec": open_stats["seqs_per_sec"],
+        "plain_per_call_seqs_per_sec": plain,
+        "served_vs_plain": cap["seqs_per_sec"] / plain if plain else None,
+    }
+
+
+def ism_explain_leg(sv, svl, coef, n=512):
+    """Config 4: ISM (all 3 x 1000 substitutions) and GkmExplain hypothetical
+    attributions of n x 1,000 bp sequences on the 72k-SV t=2 model."""
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+    import gkmsvm_lite_b200.synthetic as syn
+
+    model = gk.GkmSVM(sv, coef, 0.0, "gkm_esttrunc", PARAMS_T2, sv_lengths=svl).cuda()
+    x = syn.config4_queries()[:n]
+    out = {"workload": f"config4: {n} x 1,000 bp, 72,000-SV t=2 model"}
+    for name, fn in (("ism", lambda xs: gk.ism(model, xs)),
+                     ("explain_hypothetical", lambda xs: gk.gkmexplain(model, xs, mode="hypothetical",
+                                                                      batch_size=n))):
+        fn(x[:8])
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn(x)
+        b.record()
+        torch.cuda.synchronize()
+        out[name] = {"value": n / (a.elapsed_time(b) / 1e3), "unit": "seqs/sec"}
+    out["ism_path"] = "l-mer table + fused mutant self-kernels" if model._lmer_table is not None else "index"
+    return out
+
+
 def run_b200(args):
     import torch
 
@@ -350,6 +463,8 @@ def run_b200(args):
             result["t2_table"] = {"value": 3 * B / (a.elapsed_time(b) / 1e3), "unit": "seqs/sec",
                                   "table_build_s": tb}
             if world == 1:
+                result["serving"] = serving_leg(sv, svl, coef)
+                result["ism_explain"] = ism_explain_leg(sv, svl, coef)
                 result["cpu_baseline"] = cpu_baseline((sv, svl, coef), model._sv_diag().cpu().numpy(), xq, xl,
                                                       PARAMS_T3)
     if rank == 0:
