@@ -51,6 +51,7 @@ SIGNATURES = {
     "gkm_pack": [SPEC, P, P, I64, I64, P, P, P, P],
     "gkm_self_kernel": [SPEC, P, P, P, I64, I64, P, P, P],
     "gkm_join_pairwise": [SPEC, P, P, I64, I64, P, P, P, I64, I64, P, P, P],
+    "gkm_dense_pairwise": [SPEC, P, P, I64, I64, P, P, P, I64, I64, P, P, P, P],
     "gkm_index_create": [SPEC, P, P, P, I64, I64, P, I32, I32, P, P],
     "gkm_index_free": [P],
     "gkm_index_info": [P, P, P, P, P],

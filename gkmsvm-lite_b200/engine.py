@@ -88,6 +88,56 @@ def join_pairwise(spec: Spec, bx, cx, by, ry, cy, raw: bool = True, profile: boo
     return out, prof
 
 
+def dense_applies(spec: Spec) -> bool:
+    """The tensor-core form needs 0 <= dmax < l <= 15."""
+    b = spec.base
+    return 0 <= b.dmax < b.l <= 15
+
+
+def dense_pairwise(spec: Spec, bx, cx, by, ry, cy, raw: bool = True, profile: bool = False,
+                   check: bool = True):
+    """join_pairwise's results from the tensor-core kernel.  check: read the
+    kernel's error flag back (synchronises) and raise if an MMA timed out."""
+    B, Wx = bx.shape
+    S, Wy = by.shape
+    out = torch.empty((B, S), dtype=torch.float64, device=bx.device) if raw else None
+    prof = torch.empty((B, S, spec.base.l + 1), dtype=torch.int64, device=bx.device) if profile else None
+    err = torch.zeros(1, dtype=torch.int32, device=bx.device)
+    call("gkm_dense_pairwise", spec.ref, ptr(bx), ptr(cx), B, Wx, ptr(by), ptr(ry), ptr(cy), S, Wy,
+         ptr(out), ptr(prof), ptr(err), _st())
+    if check and int(err.item()) != 0:
+        raise _lib.GkmError("tensor-core pairwise: an MMA did not complete within its wait limit")
+    return out, prof
+
+
+# Pairwise method: "join" (warp ballot/popc over window pairs), "dense"
+# (tensor-core one-hot product), or "auto": dense where it applies, the query
+# rows have at least DENSE_MIN_WINDOWS windows and the neighbourhood reaches
+# DENSE_MIN_DMAX mismatches (the join's cost grows with the levels it counts;
+# the tensor-core product's does not).
+PAIRWISE_METHOD = "auto"
+DENSE_MIN_WINDOWS = 64
+DENSE_MIN_DMAX = 6
+
+
+def choose_pairwise(spec: Spec, Wx: int) -> str:
+    if dense_applies(spec) and Wx >= DENSE_MIN_WINDOWS and spec.base.dmax >= DENSE_MIN_DMAX:
+        return "dense"
+    return "join"
+
+
+def pairwise(spec: Spec, bx, cx, by, ry, cy, raw: bool = True, profile: bool = False, method: str | None = None):
+    """Pairwise K_raw / profiles through the join or the tensor-core kernel."""
+    method = method or PAIRWISE_METHOD
+    if method == "auto":
+        method = choose_pairwise(spec, int(bx.shape[1]))
+    if method == "dense":
+        return dense_pairwise(spec, bx, cx, by, ry, cy, raw, profile)
+    if method != "join":
+        raise ValueError(f"pairwise method must be 'auto', 'join' or 'dense', got {method!r}")
+    return join_pairwise(spec, bx, cx, by, ry, cy, raw, profile)
+
+
 def masks_tensor(base, device) -> torch.Tensor:
     m = base.masks()
     return torch.from_numpy(m.view(np.int32).copy()).to(device)

@@ -173,7 +173,7 @@ def mutation_impact(model, ref, alt, *, ref_lengths=None, alt_lengths=None, batc
             kb, _ = index.pairwise(fwd, counts)
         else:
             by, ry, cy = model._sv_packed()
-            kb, _ = engine.join_pairwise(spec, fwd, counts, by, ry, cy)
+            kb, _ = engine.pairwise(spec, fwd, counts, by, ry, cy)
         ds = model._sv_diag() if base.normalize else None
         parts.append(engine.impact(kb, n, dr, ds, model._sv_coef(), gamma, rbf))
     out = torch.cat(parts)[:, None]

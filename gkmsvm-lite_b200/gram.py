@@ -57,7 +57,7 @@ def compute_gram(kernel, X, Y=None, *, chunk_size=1000, verbose=False, out=None,
     else:
         step = max(1, _MAX_BLOCK_BYTES // (8 * M))
         for s in range(0, N, step):
-            r, _ = engine.join_pairwise(spec, bx[s:s + step], cx[s:s + step], by, ry, cy)
+            r, _ = engine.pairwise(spec, bx[s:s + step], cx[s:s + step], by, ry, cy)
             raw[s:s + step] = r
     rbf = isinstance(kernel, RbfKernel)
     gram = engine.gram_finish(raw, dx, dy, kernel.gamma if rbf else 0.0, rbf, symmetric)

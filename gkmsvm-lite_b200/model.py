@@ -265,7 +265,7 @@ class GkmSVM:
         out = []
         ds = self._sv_diag() if base.normalize else None
         for s in range(0, fwd.shape[0], step):
-            raw, _ = engine.join_pairwise(spec, fwd[s:s + step], counts[s:s + step], by, ry, cy)
+            raw, _ = engine.pairwise(spec, fwd[s:s + step], counts[s:s + step], by, ry, cy)
             out.append(engine.raw_score(raw, None if dx is None else dx[s:s + step], ds, self._sv_coef(),
                                         gamma, rbf, self.bias))
         return torch.cat(out)

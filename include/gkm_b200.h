@@ -80,6 +80,19 @@ int gkm_join_pairwise(const gkm_spec *spec, const uint32_t *bx, const int32_t *c
                       const int32_t *cy, int64_t S, int64_t Wy, double *raw,
                       uint64_t *profile, gkm_stream_t stream);
 
+/* The same pairwise K_raw and profiles as gkm_join_pairwise, computed on the
+ * tensor cores: match counts of 128 query windows x 256 column windows as one
+ * int8 one-hot product (tcgen05.mma kind::i8, int32 accumulators in tensor
+ * memory), pairs within dmax counted exactly in the epilogue.  Needs
+ * 0 <= dmax < l <= 15.  error (device int32, caller-zeroed): set non-zero if
+ * an MMA did not complete within its wait limit (outputs then undefined).
+ * Replaces the same pair loop as gkm_join_pairwise (kernels/packed.py:191-228,
+ * kernels/direct.py:23-42, kernels/weighted.py:47-69). */
+int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, const int32_t *cx,
+                       int64_t B, int64_t Wx, const uint32_t *by, const uint32_t *ry,
+                       const int32_t *cy, int64_t S, int64_t Wy, double *raw,
+                       uint64_t *profile, int32_t *error, gkm_stream_t stream);
+
 /* Builds the l-mer index over S columns (radix sort of the packed l-mers of
  * their forward and RC windows into per-SV-tile CSR buckets).  masks [n_masks]
  * (device): the XOR neighbour masks within dmax, each with its mismatch count

@@ -64,7 +64,7 @@ def test_self_profiles_bit_exact(small, name):
 
 
 @pytest.mark.parametrize("name", CASES)
-@pytest.mark.parametrize("path", ["join", "index"])
+@pytest.mark.parametrize("path", ["join", "dense", "index"])
 def test_pairwise_profiles_bit_exact(small, name, path):
     c = small[name]
     m = _model(c)
@@ -74,6 +74,10 @@ def test_pairwise_profiles_bit_exact(small, name, path):
     by, ry, cy = m._sv_packed()
     if path == "join":
         raw, prof = engine.join_pairwise(spec, bx, cx, by, ry, cy, profile=True)
+    elif path == "dense":
+        if not engine.dense_applies(spec):
+            pytest.skip("the tensor-core form needs dmax < l")
+        raw, prof = engine.dense_pairwise(spec, bx, cx, by, ry, cy, profile=True)
     else:
         if not m.kernel.base.index_applies():
             pytest.skip("neighbourhood too large for the index")
@@ -87,11 +91,14 @@ def test_pairwise_profiles_bit_exact(small, name, path):
 
 
 @pytest.mark.parametrize("name", CASES)
-@pytest.mark.parametrize("switch", ["auto", "index", "join", "table"])
-def test_scores_match_reference(small, name, switch):
+@pytest.mark.parametrize("switch", ["auto", "index", "join", "dense", "table"])
+def test_scores_match_reference(small, name, switch, monkeypatch):
     c = small[name]
-    sw = {"index": dict(use_lmer_table=False), "join": dict(use_lmer_table=False, use_lmer_index=False),
+    pairs = dict(use_lmer_table=False, use_lmer_index=False)
+    sw = {"index": dict(use_lmer_table=False), "join": pairs, "dense": pairs,
           "table": dict(use_lmer_table=True), "auto": {}}[switch]
+    if switch in ("join", "dense"):
+        monkeypatch.setattr(engine, "PAIRWISE_METHOD", switch)
     m = _model(c, **sw)
     with pytest.warns(UserWarning):
         got = m(c["x"], lengths=c["x_lengths"])
