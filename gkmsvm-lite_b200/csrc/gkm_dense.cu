@@ -2,21 +2,39 @@
 // tensor cores (tcgen05).
 //
 // The number of positions at which two l-mers agree is the dot product of
-// their one-hot encodings (4 bytes per position, 4l <= 64 bytes).  A CTA takes
-// 128 query windows (operand A, [128, 64] uint8) and 256 SV windows (operand B,
-// [256, 64] uint8, forward and RC windows of a chunk of SVs), and two
-// tcgen05.mma.kind::i8 instructions (K = 32 bytes each) leave the 128 x 256
-// match counts as int32 in tensor memory.  The epilogue reads them with
-// tcgen05.ld, one query window per thread, and counts every pair with at
-// least l - dmax matches into its (SV, mismatch level) -- integer and exact,
-// the same profile as the ballot/popc join and the l-mer index.
+// their one-hot encodings (4 bytes per position, 4l <= 60 bytes).  A tile of
+// 128 query windows (operand A, [128, 64] uint8) against 128 SV windows
+// (operand B, [128, 64] uint8) is two tcgen05.mma.kind::i8 instructions
+// (K = 32 bytes each) that leave the 128 x 128 match counts as int32 in tensor
+// memory.  The epilogue counts every pair with at least l - dmax matches into
+// its (SV, mismatch level) -- integer and exact, the same profile as the
+// ballot/popc join and the l-mer index.
+//
+// One CTA takes one query row against a chunk of D_CH SVs, with warp roles:
+//   - all warps first stage the row's one-hot (up to D_SEG windows: 8 A tiles)
+//     in shared memory, where it stays;
+//   - two producer warps stream the chunk's SV windows (forward, then RC,
+//     SV after SV, packed across SV boundaries) as one-hot B tiles through a
+//     double buffer, with each column's SV and window weight;
+//   - one thread issues the MMAs of every (B tile, A tile) pair, alternating
+//     between two accumulators in tensor memory, and commits each to an
+//     mbarrier;
+//   - two epilogue warpgroups, one per accumulator, read a finished
+//     accumulator into registers (tcgen05.ld, 16-bit packed), hand it straight
+//     back to the MMA thread, and only then look for pairs within dmax:
+//     an OR over each 32-column chunk and a warp ballot; the rare rows with a
+//     hit leave their values in shared scratch and the warp walks them one row
+//     at a time, a column per lane, into shared per-(SV, level) counters.
+// mbarriers hand buffers between the roles (full/empty pairs); every wait is
+// bounded in time and raises the launch's error flag when it runs out, after
+// which every role leaves its loop, the MMA thread waits (bounded) for its
+// MMAs in flight, and the tensor memory is freed.
 //
 // Operands sit in shared memory in the K-major no-swizzle core-matrix layout:
 // byte k of row r at (k / 32) * rows * 32 + (r / 8) * 256 + ((k % 32) / 16) *
 // 128 + (r % 8) * 16 + k % 16, so one MMA's operand is [rows, 32 bytes] with
 // core matrices 8 rows x 16 bytes, 128 bytes apart along K and 256 bytes apart
-// along rows.  One elected thread issues the MMAs and commits them to an
-// mbarrier; every wait on it is bounded and sets an error flag on timeout.
+// along rows.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -24,14 +42,41 @@
 
 namespace {
 
-constexpr int DM = 128;          // query windows per tile (MMA M)
-constexpr int DN = 256;          // SV windows per tile (MMA N)
-constexpr int DKB = 64;          // one-hot bytes per window (4l <= 64)
-constexpr int D_THREADS = 128;   // one warpgroup: a TMEM lane quadrant per warp
-constexpr int D_SV_CHUNK = 8;    // SVs per CTA
+constexpr int DM = 128;            // query windows per A tile (MMA M)
+constexpr int DN = 128;            // SV windows per B tile (MMA N)
+constexpr int DKB = 64;            // one-hot bytes per window
+constexpr int D_SEG = 1024;        // query windows staged at a time (8 A tiles)
+constexpr int D_CH = 16;           // SVs per CTA
 constexpr int D_LEVELS = 16;
-constexpr uint32_t D_TMEM_COLS = 256;
-constexpr uint64_t D_WAIT_NS = 1000000000ull;  // give up on an MMA after 1 s
+constexpr int D_EPI_WARPS = 8;     // warps 0..7: warpgroup w / 4 drains accumulator w / 4,
+                                   // warp w reads TMEM lane quadrant w % 4
+constexpr int D_PROD_WARPS = 2;    // warps 8..9
+constexpr int D_MMA_WARP = D_EPI_WARPS + D_PROD_WARPS;  // warp 10
+constexpr int D_THREADS = (D_MMA_WARP + 1) * 32;
+constexpr uint32_t D_TMEM_COLS = 2 * DN;  // two accumulators
+constexpr int A_TILE = DM * DKB;   // 8 KB
+constexpr int B_TILE = DN * DKB;   // 8 KB
+constexpr uint64_t D_WAIT_NS = 1000000000ull;  // give up on a hand-off after 1 s
+
+// dynamic shared memory
+constexpr int OFF_A = 0;
+constexpr int OFF_B = OFF_A + D_SEG * DKB;
+constexpr int OFF_COLSV = OFF_B + 2 * B_TILE;
+constexpr int OFF_COLW = OFF_COLSV + 2 * DN;
+constexpr int OFF_CNT = OFF_COLW + 2 * DN;
+constexpr int OFF_PRE = OFF_CNT + D_CH * D_LEVELS * 8;
+constexpr int D_SCR_STRIDE = 20;   // words per lane (16 used; 20 keeps 16-byte stores conflict-free)
+constexpr int OFF_SCR = (OFF_PRE + (D_CH + 1) * 4 + 15) & ~15;
+constexpr int D_SMEM_USED = OFF_SCR + D_EPI_WARPS * 32 * D_SCR_STRIDE * 4;
+// requested: more than a third of the SM's shared memory, so at most two CTAs
+// share an SM and their 2 x 256 tensor-memory columns always fit its 512
+constexpr int D_SMEM = 106 * 1024;
+static_assert(OFF_CNT % 16 == 0, "counter alignment");
+static_assert(D_SMEM_USED <= D_SMEM, "shared memory layout");
+static_assert(3 * (D_SMEM + 2048) > 228 * 1024, "at most two CTAs per SM");
+
+// mbarriers (static shared memory)
+enum { BAR_BFULL = 0, BAR_BEMPTY = 2, BAR_TFULL = 4, BAR_TEMPTY = 6, BAR_DONE = 8, N_BARS = 9 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -47,7 +92,7 @@ __device__ __forceinline__ uint64_t make_sdesc(uint32_t saddr, uint32_t lbo, uin
 }
 
 // instruction descriptor: kind::i8, unsigned A and B, int32 accumulate, K-major
-// A and B, M = 128, N = 256
+// A and B, M = DM, N = DN
 __host__ __device__ constexpr uint32_t make_idesc()
 {
     return (2u << 4)                      // D format: S32
@@ -86,23 +131,51 @@ __device__ __forceinline__ uint64_t global_ns()
     return t;
 }
 
-// waits for the mbarrier phase with parity `phase` to complete; false after
-// D_WAIT_NS of wall time
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase)
+__device__ __forceinline__ bool bar_test(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase of `bar` with parity `parity` to complete.  False when
+// another role has aborted (*abort set) or after D_WAIT_NS, which sets *abort
+// and the launch's error flag.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, volatile int *abort, int *error)
 {
     const uint64_t t0 = global_ns();
     for (;;) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(bar), "r"(phase)
-            : "memory");
-        if (ok) return true;
-        if (global_ns() - t0 > D_WAIT_NS) return false;
+        if (bar_test(bar, parity)) return true;
+        if (*abort) return false;
+        if (global_ns() - t0 > D_WAIT_NS) {
+            *abort = 1;
+            atomicOr(error, 1);
+            return false;
+        }
     }
+}
+
+__device__ __forceinline__ void bar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// 32 columns of this warp's 32 TMEM lanes, two 16-bit values per register
+// (column 2i in the low half of v[i], column 2i + 1 in the high half)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t *v)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.pack::16b.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+        "[%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
 }
 
 struct DenseArgs {
@@ -120,17 +193,20 @@ struct DenseArgs {
     int *error;
 };
 
-__global__ void __launch_bounds__(D_THREADS) dense_join_kernel(DenseArgs a)
+__global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
 {
     extern __shared__ __align__(1024) uint8_t sm[];
-    uint8_t *smA = sm;                                     // [DM, 64] core-matrix layout (8 KB)
-    uint8_t *smB = sm + DM * DKB;                          // [DN, 64] (16 KB)
-    uint16_t *col_sv = (uint16_t *)(smB + DN * DKB);       // [DN] SV of each B column (0xFFFF: none)
-    uint8_t *col_w = (uint8_t *)(col_sv + DN);             // [DN] its window weight
-    unsigned long long *cnt = (unsigned long long *)(((uintptr_t)(col_w + DN) + 15) & ~(uintptr_t)15);
-    __shared__ __align__(8) uint64_t mbar;
+    uint8_t *smA = sm + OFF_A;                 // [D_SEG / DM] A tiles, core-matrix layout
+    uint8_t *smB = sm + OFF_B;                 // [2] B tiles
+    uint8_t *col_sv = sm + OFF_COLSV;          // [2][DN] chunk-local SV of each B column
+    uint8_t *col_w = sm + OFF_COLW;            // [2][DN] its window weight
+    unsigned long long *cnt = (unsigned long long *)(sm + OFF_CNT);  // [D_CH][D_LEVELS]
+    int *pre = (int *)(sm + OFF_PRE);          // [D_CH + 1] window offsets of the chunk's SVs
+    uint32_t *scratch = (uint32_t *)(sm + OFF_SCR);  // [epilogue warp][lane][D_SCR_STRIDE]
+    __shared__ __align__(8) uint64_t bars[N_BARS];
     __shared__ uint32_t tmem_base;
-    __shared__ int failed;
+    __shared__ int abort_flag;
+    volatile int *abort = &abort_flag;
 
     const gkm_spec &sp = a.spec;
     const int l = sp.l, dmax = sp.dmax;
@@ -140,20 +216,30 @@ __global__ void __launch_bounds__(D_THREADS) dense_join_kernel(DenseArgs a)
     // window or a missing column accumulate 0.
     const uint32_t bias_b = 32u - (uint32_t)(l - dmax);
     const int64_t b = blockIdx.x;
-    const int64_t s_lo = (int64_t)blockIdx.y * D_SV_CHUNK;
-    const int nsv = (int)min((int64_t)D_SV_CHUNK, a.S - s_lo);
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int64_t s_lo = (int64_t)blockIdx.y * D_CH;
+    const int nsv = (int)min((int64_t)D_CH, a.S - s_lo);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool has_rc = sp.include_rc && a.ry != nullptr;
+    const uint32_t bar0 = smem_addr(bars);
+    auto bar = [&](int k) { return bar0 + 8u * (uint32_t)k; };
 
-    // an earlier CTA gave up on an MMA: skip the work (the outputs are
+    // an earlier CTA gave up on a hand-off: skip the work (the outputs are
     // undefined and the host raises), so a failed launch ends quickly.  One
     // read, shared, so the whole block takes the same branch.
-    if (tid == 0) failed = *(volatile int *)a.error != 0;
+    if (tid == 0) abort_flag = *(volatile int *)a.error != 0;
     __syncthreads();
-    if (failed) return;
-    for (int k = tid; k < D_SV_CHUNK * D_LEVELS; k += D_THREADS) cnt[k] = 0;
+    if (abort_flag) return;
+
+    for (int k = tid; k < D_CH * D_LEVELS; k += D_THREADS) cnt[k] = 0;
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar)));
+        pre[0] = 0;
+        for (int s = 0; s < nsv; s++) pre[s + 1] = pre[s] + (has_rc ? 2 : 1) * a.cy[s_lo + s];
+        // B buffers: filled by each producer warp, emptied by every epilogue
+        // warp; accumulators: filled by the MMA commit, emptied by the four
+        // warps of their warpgroup
+        const uint32_t counts[N_BARS] = {D_PROD_WARPS, D_PROD_WARPS, D_EPI_WARPS, D_EPI_WARPS, 1, 1, 4, 4, 1};
+        for (int k = 0; k < N_BARS; k++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar(k)), "r"(counts[k]));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -165,120 +251,175 @@ __global__ void __launch_bounds__(D_THREADS) dense_join_kernel(DenseArgs a)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
-
+    const int ny_total = pre[nsv];
+    const int NB = (ny_total + DN - 1) / DN;
     const int nx = a.cx[b];
-    // SV windows of this chunk, listed SV by SV: forward windows then RC ones
-    int ny_total = 0;
-    for (int s = 0; s < nsv; s++) ny_total += (has_rc ? 2 : 1) * a.cy[s_lo + s];
     const uint32_t idesc = make_idesc();
-    uint32_t phase = 0;
+    uint32_t g_base = 0, t_base = 0;  // B tiles and tile pairs of earlier segments
 
-    for (int c0 = 0; c0 < ny_total && !failed; c0 += DN) {
-        // B tile: column j = SV window c0 + j
-        for (int j = tid; j < DN; j += D_THREADS) {
-            int t = c0 + j, s = 0;
-            uint32_t w = GKM_PAD;
-            uint16_t sv = 0xFFFF;
-            uint8_t wt = 0;
-            if (t < ny_total) {
-                for (; s < nsv; s++) {
-                    const int n2 = (has_rc ? 2 : 1) * a.cy[s_lo + s];
-                    if (t < n2) break;
-                    t -= n2;
-                }
-                const int64_t sg = s_lo + s;
-                const int ny = a.cy[sg];
-                if (t < ny) {
-                    w = a.by[sg * a.Wy + t];
-                    wt = sp.weighted ? (uint8_t)gkm_wt(sp.wd, ny, t) : 1;
-                } else {  // RC of forward window ny - 1 - (t - ny)
-                    const int f = ny - 1 - (t - ny);
-                    w = a.ry[sg * a.Wy + (a.Wy - 1 - f)];
-                    wt = sp.weighted ? (uint8_t)gkm_wt(sp.wd, ny, f) : 1;
-                }
-                sv = (uint16_t)s;
-            }
-            onehot_row(smB, j, DN, w, l, bias_b);
-            col_sv[j] = sv;
-            col_w[j] = wt;
+    for (int seg0 = 0; seg0 < nx && NB > 0; seg0 += D_SEG) {
+        const int nseg = min(D_SEG, nx - seg0);
+        const int NA = (nseg + DM - 1) / DM;
+        // every warp: this segment's A tiles (rows past the row's end: zero)
+        for (int r = tid; r < NA * DM; r += D_THREADS) {
+            const uint32_t w = r < nseg ? a.bx[b * a.Wx + seg0 + r] : GKM_PAD;
+            onehot_row(smA + (r / DM) * A_TILE, r % DM, DM, w, l, 1u);
         }
-        for (int r0 = 0; r0 < nx && !failed; r0 += DM) {
-            // A tile: this thread's query window
-            {
-                const int i = r0 + tid;
-                const uint32_t w = i < nx ? a.bx[b * a.Wx + i] : GKM_PAD;
-                onehot_row(smA, tid, DM, w, l, 1u);
-            }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("tcgen05.fence::before_thread_sync;");
-            __syncthreads();
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            if (tid == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+
+        if (warp < D_EPI_WARPS) {
+            // ---- epilogue: warpgroup eg drains the accumulator of the tiles t
+            // with t % 2 == eg; TMEM lane quadrant `quad`, one query window per thread
+            const uint32_t eg = (uint32_t)(warp >> 2);
+            const int quad = warp & 3;
+            uint32_t *scr = scratch + warp * 32 * D_SCR_STRIDE;
+            for (int bt = 0; bt < NB; bt++) {
+                const uint32_t g = g_base + bt, buf = g & 1u;
+                const uint8_t *csv = col_sv + buf * DN, *cw = col_w + buf * DN;
+                // wait for this B tile to be filled even when none of its tiles is
+                // ours: the release below must not count toward an earlier
+                // phase of the buffer while the other warpgroup still reads it
+                bool ok = __all_sync(GKM_FULL, bar_wait(bar(BAR_BFULL + buf), (g >> 1) & 1u, abort, a.error));
+                if (!ok) break;
+                for (int at = 0; at < NA; at++) {
+                    const uint32_t t = t_base + (uint32_t)(bt * NA + at), slot = t & 1u;
+                    if (slot != eg) continue;
+                    ok = __all_sync(GKM_FULL, bar_wait(bar(BAR_TFULL + slot), (t >> 1) & 1u, abort, a.error));
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                    // the whole accumulator row in 64 registers (values < 48), then
+                    // the accumulator goes back to the MMA thread before any counting
+                    uint32_t p[DN / 2];
+                    const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + slot * DN;
 #pragma unroll
-                for (int kb = 0; kb < 2; kb++) {
-                    const uint64_t da = make_sdesc(smem_addr(smA) + kb * DM * 32, 128, 256);
-                    const uint64_t db = make_sdesc(smem_addr(smB) + kb * DN * 32, 128, 256);
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                        "l"(da), "l"(db), "r"(idesc), "r"(kb));
-                }
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                    smem_addr(&mbar)));
-            }
-            if (!mbar_wait(smem_addr(&mbar), phase)) {
-                failed = 1;
-                atomicOr(a.error, 1);
-            }
-            phase ^= 1u;
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            __syncthreads();
-            if (failed) break;
-            // epilogue: this thread's row (TMEM lane 32 * warp + lane)
-            const int i = r0 + tid;
-            const uint64_t wx = (i < nx && sp.weighted) ? gkm_wt(sp.wd, nx, i) : 1;
-#pragma unroll 1
-            for (int c = 0; c < DN / 32; c++) {
-                uint32_t v[32];
-                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32);
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
-                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
-                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                    : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                uint32_t any = 0;
+                    for (int k = 0; k < DN / 32; k++) tmem_ld16(taddr + (uint32_t)(32 * k), p + 16 * k);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    asm volatile("tcgen05.fence::before_thread_sync;");
+                    __syncwarp();
+                    if (lane == 0) bar_arrive(bar(BAR_TEMPTY + slot));
+
+                    const int r = at * DM + quad * 32 + lane;
+                    const uint32_t wx = (sp.weighted && r < nseg) ? gkm_wt(sp.wd, nx, seg0 + r) : 1u;
 #pragma unroll
-                for (int j = 0; j < 32; j++) any |= v[j];
-                if (any & 32u) {  // some pair of this row is within dmax here
+                    for (int k = 0; k < DN / 32; k++) {
+                        uint32_t o = 0;
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        const int col = c * 32 + j;
-                        if (v[j] & 32u)  // mismatches l - (v - bias_b)
-                            atomicAdd(&cnt[col_sv[col] * D_LEVELS + (32 + dmax - (int)v[j])],
-                                      (unsigned long long)(wx * col_w[col]));
+                        for (int i = 0; i < 16; i++) o |= p[16 * k + i];
+                        const bool mine = (o & 0x00200020u) != 0;  // a pair of this row within dmax
+                        unsigned rows = __ballot_sync(GKM_FULL, mine);
+                        if (rows == 0) continue;  // warp-uniform: the common case
+                        // rows with a hit leave their 32 values in the warp's scratch;
+                        // the warp then takes them one row at a time, a column per lane
+                        if (mine) {
+#pragma unroll
+                            for (int i = 0; i < 4; i++)
+                                *(uint4 *)(scr + lane * D_SCR_STRIDE + 4 * i) =
+                                    make_uint4(p[16 * k + 4 * i], p[16 * k + 4 * i + 1], p[16 * k + 4 * i + 2],
+                                               p[16 * k + 4 * i + 3]);
+                        }
+                        __syncwarp();
+                        const int col = 32 * k + lane;
+                        const uint32_t csv_l = csv[col], cw_l = cw[col];
+                        while (rows) {
+                            const int q = __ffs(rows) - 1;
+                            rows &= rows - 1;
+                            const uint32_t word = scr[q * D_SCR_STRIDE + (lane >> 1)];
+                            const uint32_t v = (lane & 1) ? (word >> 16) : (word & 0xFFFFu);
+                            const uint32_t wq = __shfl_sync(GKM_FULL, wx, q);
+                            if (v & 32u)  // mismatches l - (v - bias_b)
+                                atomicAdd(&cnt[csv_l * D_LEVELS + (32 + dmax - (int)v)],
+                                          (unsigned long long)(wq * cw_l));
+                        }
+                        __syncwarp();  // scratch is rewritten by the next chunk
                     }
                 }
-                __syncwarp();  // the next tcgen05.ld is warp-aligned
+                if (!ok) break;
+                __syncwarp();  // B tile's column tables no longer read: hand the buffer back
+                if (lane == 0) bar_arrive(bar(BAR_BEMPTY + buf));
             }
-            asm volatile("tcgen05.fence::before_thread_sync;");
-            __syncthreads();
-            asm volatile("tcgen05.fence::after_thread_sync;");
+        } else if (warp < D_MMA_WARP) {
+            // ---- producers: B tiles, DN columns each
+            const int pl = tid - D_EPI_WARPS * 32;  // 0 .. D_PROD_WARPS * 32 - 1
+            for (int bt = 0; bt < NB; bt++) {
+                const uint32_t g = g_base + bt, buf = g & 1u;
+                if (g >= 2) {
+                    // each producer warp waits and decides alone (no barrier
+                    // joins the two warps, so one leaving never blocks the other)
+                    const bool ok = bar_wait(bar(BAR_BEMPTY + buf), ((g >> 1) - 1) & 1u, abort, a.error);
+                    if (!__all_sync(GKM_FULL, ok)) break;
+                }
+                for (int j = pl; j < DN; j += D_PROD_WARPS * 32) {
+                    const int t = bt * DN + j;
+                    uint32_t w = GKM_PAD;
+                    int s = 0;
+                    uint8_t wt = 0;
+                    if (t < ny_total) {
+                        while (t >= pre[s + 1]) s++;
+                        const int u = t - pre[s];
+                        const int64_t sg = s_lo + s;
+                        const int ny = a.cy[sg];
+                        if (u < ny) {
+                            w = a.by[sg * a.Wy + u];
+                            wt = sp.weighted ? (uint8_t)gkm_wt(sp.wd, ny, u) : 1;
+                        } else {  // RC of forward window ny - 1 - (u - ny)
+                            const int f = ny - 1 - (u - ny);
+                            w = a.ry[sg * a.Wy + (a.Wy - 1 - f)];
+                            wt = sp.weighted ? (uint8_t)gkm_wt(sp.wd, ny, f) : 1;
+                        }
+                    }
+                    onehot_row(smB + buf * B_TILE, j, DN, w, l, bias_b);
+                    col_sv[buf * DN + j] = (uint8_t)s;
+                    col_w[buf * DN + j] = wt;
+                }
+                // this warp's columns are written: one arrival per producer warp
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) bar_arrive(bar(BAR_BFULL + buf));
+            }
+        } else if (lane == 0) {
+            // ---- MMA issue: every (B tile, A tile) pair, accumulators alternating
+            bool ok = true;
+            for (int bt = 0; bt < NB && ok; bt++) {
+                const uint32_t g = g_base + bt, buf = g & 1u;
+                ok = bar_wait(bar(BAR_BFULL + buf), (g >> 1) & 1u, abort, a.error);
+                for (int at = 0; at < NA && ok; at++) {
+                    const uint32_t t = t_base + (uint32_t)(bt * NA + at), slot = t & 1u;
+                    if (t >= 2) ok = bar_wait(bar(BAR_TEMPTY + slot), ((t >> 1) - 1) & 1u, abort, a.error);
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+                    for (int kb = 0; kb < 2; kb++) {
+                        const uint64_t da = make_sdesc(smem_addr(smA + at * A_TILE) + kb * DM * 32, 128, 256);
+                        const uint64_t db = make_sdesc(smem_addr(smB + buf * B_TILE) + kb * DN * 32, 128, 256);
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + slot * DN),
+                            "l"(da), "l"(db), "r"(idesc), "r"(kb));
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                        bar(BAR_TFULL + slot)));
+                }
+            }
         }
-        __syncthreads();  // B is rebuilt next
+        g_base += (uint32_t)NB;
+        t_base += (uint32_t)(NB * NA);
+        __syncthreads();  // segment done (or abandoned): A is restaged next
+        if (abort_flag) break;
     }
-    // a timed-out MMA may still be in flight: one more bounded wait before its
-    // accumulator columns are released
-    if (failed && tid == 0) mbar_wait(smem_addr(&mbar), phase ^ 1u);
+    // every MMA issued has completed before its accumulator columns are
+    // released (bounded: on a stuck MMA the wait runs out and the error is set)
+    if (warp == D_MMA_WARP && lane == 0) {
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            bar(BAR_DONE)));
+        int ignore = 0;
+        bar_wait(bar(BAR_DONE), 0u, &ignore, a.error);
+    }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(D_TMEM_COLS));
-    if (failed) return;
+    if (abort_flag) return;
     for (int s = tid; s < nsv; s += D_THREADS) {
         const int64_t sg = s_lo + s;
         double k = 0.0;
@@ -302,8 +443,9 @@ extern "C" int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, cons
     if (spec->weighted && (!spec->wd || spec->wd_len < 1)) return gkm_fail(GKM_ERR_INVALID, "weighted spec without weights");
     if (B == 0 || S == 0) return GKM_OK;
     if (!bx || !cx || !by || !cy || !error) return gkm_fail(GKM_ERR_INVALID, "null argument");
-    if (B > 0x7FFFFFFFLL || (S + D_SV_CHUNK - 1) / D_SV_CHUNK > 65535)
+    if (B > 0x7FFFFFFFLL || (S + D_CH - 1) / D_CH > 65535)
         return gkm_fail(GKM_ERR_UNSUPPORTED, "too many rows or columns for one dense launch");
+    if ((int64_t)D_CH * 2 * Wy > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "columns too long for one dense launch");
     DenseArgs a;
     a.spec = *spec;
     a.bx = bx;
@@ -317,12 +459,9 @@ extern "C" int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, cons
     a.raw = raw;
     a.profile = profile;
     a.error = error;
-    // operands + column tables + counters; 100 KB keeps at most two CTAs per
-    // SM, so their 256 TMEM columns each always fit the SM's 512
-    size_t smem = 100 * 1024;
-    cudaFuncSetAttribute(dense_join_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid((unsigned)B, (unsigned)((S + D_SV_CHUNK - 1) / D_SV_CHUNK));
-    dense_join_kernel<<<grid, D_THREADS, smem, (cudaStream_t)stream>>>(a);
-    GKM_CHECK_LAUNCH("dense_join");
+    cudaFuncSetAttribute(dense_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, D_SMEM);
+    dim3 grid((unsigned)B, (unsigned)((S + D_CH - 1) / D_CH));
+    dense_pairs_kernel<<<grid, D_THREADS, D_SMEM, (cudaStream_t)stream>>>(a);
+    GKM_CHECK_LAUNCH("dense_pairs");
     return GKM_OK;
 }

@@ -1,8 +1,9 @@
 """GPU parity of the tensor-core pairwise kernel (gkm_dense_pairwise): mismatch
 profiles bit-exact against the oracle, and K_raw bit-identical to the warp
 join, on shapes that cross its tile edges -- query rows over several 128-window
-tiles, column sets over several 256-window tiles, SV counts that are not a
-multiple of its 8-SV chunk, rows without windows, l from 1 to 15 and dmax up to
+tiles and over several 1,024-window staged segments, column sets over many
+128-window tiles, SV counts that are not a multiple of its 16-SV chunk, rows
+without windows, l from 1 to 15 and dmax up to
 l - 1, weighted and unweighted, with and without reverse complements."""
 
 import numpy as np
@@ -27,6 +28,8 @@ CASES = {
                      [120, 9, 300, 44, 45, 46, 47, 48, 49]),
     "wgkmrbf_l10": ("wgkmrbf", dict(L=10, k=6, d=3, gamma=2.0, M=30, H=10.0), [257, 130, 64],
                     [256, 129, 128, 127, 10, 260, 200, 64, 63, 140, 150, 160, 170, 180, 190, 120, 110]),
+    "esttrunc_l11_segments": ("gkm_esttrunc", dict(L=11, k=7, d=3), [2500, 1100, 1034, 1035, 40],
+                              [300, 64, 1030, 2100]),
     "estfull_l8_many": ("gkm_estfull", dict(L=8, k=4, d=2), [100, 100, 100, 100],
                         [50 + 7 * i for i in range(41)]),
 }
