@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--queries", type=int, default=100000)
     ap.add_argument("--no-extras", action="store_true", help="skip t=2, plain-call and CPU legs")
+    ap.add_argument("--leg", default="all", choices=["all", "gram"],
+                    help="gram: run only the Gram-matrix leg (one GPU) and print its JSON")
+    ap.add_argument("--gram-n", type=int, default=4000, help="sequences of the Gram-matrix leg")
     return ap.parse_args()
 
 
@@ -300,6 +303,67 @@ def ism_explain_leg(sv, svl, coef, n=512):
     return out
 
 
+def gram_leg(n=4000, forms=("index", "dense", "join")):
+    """Config 2: the normalised symmetric Gram matrix of n sequences (lengths
+    log-uniform in 100..1000 bp), t=4 wgkm l=11 k=7 d=3, through
+    gkmsvm_lite_b200.compute_gram (host codes in, host matrix out); beside it
+    the raw pairwise kernel K_raw [n, n] of each device form on the same packed
+    windows, with its pair count: the l-mer index (lookups and hits), the
+    tensor-core one-hot product and the warp join (every window pair)."""
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+    import gkmsvm_lite_b200.synthetic as syn
+    from gkmsvm_lite_b200 import engine
+
+    x, xl = syn.config2(n=n)
+    k = gk.CenterWeightedGkmKernel(11, 7, d=3)
+    gk.compute_gram(k, x[:64], lengths=xl[:64])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    gk.compute_gram(k, x, lengths=xl)
+    e2e = time.perf_counter() - t0
+    dev = torch.device("cuda", torch.cuda.current_device())
+    spec = engine.Spec(k.base, dev)
+    bx, rx, cx = engine.pack(spec, torch.from_numpy(x).to(dev), xl)
+    n_win = int(cx.sum().item())
+    pairs = n_win * 2 * n_win
+    out = {"workload": f"config2: {n} sequences 100-1000 bp log-uniform, t=4 wgkm l=11 k=7 d=3",
+           "compute_gram_s": e2e, "compute_gram_path": "index" if k.base.index_applies(2 * n_win) else "pairwise",
+           "windows": n_win, "window_pairs": pairs, "raw_ms": {}}
+    ref = None
+    for form in forms:
+        if form == "index":
+            ix = engine.DeviceIndex(spec, bx, rx, cx, engine.masks_tensor(k.base, dev))
+            fn = lambda: ix.pairwise(bx, cx)[0]
+        elif form == "dense":
+            if not engine.dense_applies(spec):
+                continue
+            fn = lambda: engine.dense_pairwise(spec, bx, cx, bx, rx, cx, check=False)[0]
+        else:
+            fn = lambda: engine.join_pairwise(spec, bx, cx, bx, rx, cx)[0]
+        if form == "dense":  # warm-up call reads its error flag back
+            engine.dense_pairwise(spec, bx, cx, bx, rx, cx)
+        else:
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        r = fn()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        same = None
+        if ref is None:
+            ref = r
+        else:
+            same = bool(torch.equal(r, ref))
+        out["raw_ms"][form] = {"ms": ms, "Gpairs_per_s": pairs / ms / 1e6, "identical_to_first": same}
+        if form == "index":
+            ix.close()
+    return out
+
+
 def run_b200(args):
     import torch
 
@@ -465,6 +529,7 @@ def run_b200(args):
             if world == 1:
                 result["serving"] = serving_leg(sv, svl, coef)
                 result["ism_explain"] = ism_explain_leg(sv, svl, coef)
+                result["gram"] = gram_leg(args.gram_n)
                 result["cpu_baseline"] = cpu_baseline((sv, svl, coef), model._sv_diag().cpu().numpy(), xq, xl,
                                                       PARAMS_T3)
     if rank == 0:
@@ -480,6 +545,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.leg == "gram":
+        print(json.dumps(gram_leg(args.gram_n)), flush=True)
+        return 0
     return run_b200(args)
 
 

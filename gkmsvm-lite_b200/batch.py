@@ -15,6 +15,9 @@ self-kernel plus W lookups per row), also captured.
 
 from __future__ import annotations
 
+import gc
+import weakref
+
 import numpy as np
 import torch
 
@@ -44,7 +47,11 @@ class _Graph:
         self.lengths = torch.zeros(rows, dtype=torch.int64, device=dev)
         self.out = torch.empty(rows, dtype=torch.float64, device=dev)
         self.graph = None
-        self.scorer = scorer
+        self._scorer = weakref.ref(scorer)  # no cycle: graphs go with their scorer
+
+    @property
+    def scorer(self):
+        return self._scorer()
 
     def _prep(self):
         s = self.scorer
@@ -82,13 +89,22 @@ class _Graph:
             self._body()
         torch.cuda.current_stream().wait_stream(side)
         # thread-local capture: other threads (a server's side stream) may keep
-        # issuing CUDA work meanwhile
-        self.g_prep = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.g_prep, capture_error_mode="thread_local"):
-            self._prep()
-        self.g_query = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.g_query, pool=self.g_prep.pool(), capture_error_mode="thread_local"):
-            self._query()
+        # issuing CUDA work meanwhile.  The cyclic garbage collector stays off
+        # while a capture is open: freeing an unreachable object that holds
+        # another CUDA graph or device memory is not permitted during capture
+        # and would invalidate it (torch.cuda.graph collects just before).
+        enabled = gc.isenabled()
+        gc.disable()
+        try:
+            self.g_prep = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.g_prep, capture_error_mode="thread_local"):
+                self._prep()
+            self.g_query = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.g_query, pool=self.g_prep.pool(), capture_error_mode="thread_local"):
+                self._query()
+        finally:
+            if enabled:
+                gc.enable()
         self.graph = True
 
     def run(self, events=None):
