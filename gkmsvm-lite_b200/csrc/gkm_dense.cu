@@ -10,25 +10,35 @@
 // its (SV, mismatch level) -- integer and exact, the same profile as the
 // ballot/popc join and the l-mer index.
 //
-// One CTA takes one query row against a chunk of D_CH SVs, with warp roles:
-//   - all warps first stage the row's one-hot (up to D_SEG windows: 8 A tiles)
-//     in shared memory, where it stays;
-//   - two producer warps stream the chunk's SV windows (forward, then RC,
-//     SV after SV, packed across SV boundaries) as one-hot B tiles through a
-//     double buffer, with each column's SV and window weight;
-//   - one thread issues the MMAs of every (B tile, A tile) pair, alternating
-//     between two accumulators in tensor memory, and commits each to an
-//     mbarrier;
-//   - two epilogue warpgroups, one per accumulator, read a finished
-//     accumulator into registers (tcgen05.ld, 16-bit packed), hand it straight
-//     back to the MMA thread, and only then look for pairs within dmax:
-//     an OR over each 32-column chunk and a warp ballot; the rare rows with a
-//     hit leave their values in shared scratch and the warp walks them one row
-//     at a time, a column per lane, into shared per-(SV, level) counters.
+// Two kernels per launch:
+//   dense_b_records  writes every B tile once to global memory as a record:
+//                    the tile's one-hot bytes already in the shared-memory
+//                    layout the MMA reads, then each column's chunk-local SV
+//                    and window weight.  The SVs are taken D_CH at a time (a
+//                    chunk); a chunk's windows -- forward then RC, SV after
+//                    SV -- are packed into consecutive tiles across SV
+//                    boundaries.
+//   dense_pairs_kernel  one CTA per (query row, SV chunk), with warp roles:
+//     - all warps first stage the row's one-hot (up to D_SEG windows: 8 A
+//       tiles) in shared memory, where it stays;
+//     - one producer thread copies the chunk's B records, one per tile, into a
+//       double buffer with cp.async.bulk (untiled, 16-byte aligned, a multiple
+//       of 16 bytes, completing on the buffer's mbarrier);
+//     - one thread issues the MMAs of every (B tile, A tile) pair, alternating
+//       between two accumulators in tensor memory, and commits each to an
+//       mbarrier;
+//     - two epilogue warpgroups, one per accumulator, read a finished
+//       accumulator into registers (tcgen05.ld, 16-bit packed), hand it
+//       straight back to the MMA thread, and only then look for pairs within
+//       dmax: an OR over each 32-column chunk and a warp ballot; the rare rows
+//       with a hit leave their values in shared scratch and the warp walks
+//       them one row at a time, a column per lane, into shared per-(SV, level)
+//       counters (32-bit where the launch's totals fit, else 64-bit).
 // mbarriers hand buffers between the roles (full/empty pairs); every wait is
 // bounded in time and raises the launch's error flag when it runs out, after
 // which every role leaves its loop, the MMA thread waits (bounded) for its
-// MMAs in flight, and the tensor memory is freed.
+// MMAs and the producer for its copies in flight, and the tensor memory is
+// freed.
 //
 // Operands sit in shared memory in the K-major no-swizzle core-matrix layout:
 // byte k of row r at (k / 32) * rows * 32 + (r / 8) * 256 + ((k % 32) / 16) *
@@ -46,32 +56,32 @@ constexpr int DM = 128;            // query windows per A tile (MMA M)
 constexpr int DN = 128;            // SV windows per B tile (MMA N)
 constexpr int DKB = 64;            // one-hot bytes per window
 constexpr int D_SEG = 1024;        // query windows staged at a time (8 A tiles)
-constexpr int D_CH = 16;           // SVs per CTA
+constexpr int D_CH = 16;           // SVs per chunk (per CTA)
 constexpr int D_LEVELS = 16;
 constexpr int D_EPI_WARPS = 8;     // warps 0..7: warpgroup w / 4 drains accumulator w / 4,
                                    // warp w reads TMEM lane quadrant w % 4
-constexpr int D_PROD_WARPS = 2;    // warps 8..9
-constexpr int D_MMA_WARP = D_EPI_WARPS + D_PROD_WARPS;  // warp 10
+constexpr int D_PROD_WARP = D_EPI_WARPS;      // warp 8 (lane 0 copies)
+constexpr int D_MMA_WARP = D_EPI_WARPS + 1;   // warp 9 (lane 0 issues)
 constexpr int D_THREADS = (D_MMA_WARP + 1) * 32;
 constexpr uint32_t D_TMEM_COLS = 2 * DN;  // two accumulators
 constexpr int A_TILE = DM * DKB;   // 8 KB
 constexpr int B_TILE = DN * DKB;   // 8 KB
+constexpr int REC = B_TILE + 2 * DN;  // B record: one-hot, column SVs, column weights
 constexpr uint64_t D_WAIT_NS = 1000000000ull;  // give up on a hand-off after 1 s
+constexpr size_t D_REC_BUDGET = (size_t)1 << 30;  // B records per launch round
+static_assert(REC % 16 == 0, "bulk copies move multiples of 16 bytes");
 
 // dynamic shared memory
 constexpr int OFF_A = 0;
 constexpr int OFF_B = OFF_A + D_SEG * DKB;
-constexpr int OFF_COLSV = OFF_B + 2 * B_TILE;
-constexpr int OFF_COLW = OFF_COLSV + 2 * DN;
-constexpr int OFF_CNT = OFF_COLW + 2 * DN;
-constexpr int OFF_PRE = OFF_CNT + D_CH * D_LEVELS * 8;
+constexpr int OFF_CNT = OFF_B + 2 * REC;
+constexpr int OFF_SCR = OFF_CNT + D_CH * D_LEVELS * 8;
 constexpr int D_SCR_STRIDE = 20;   // words per lane (16 used; 20 keeps 16-byte stores conflict-free)
-constexpr int OFF_SCR = (OFF_PRE + (D_CH + 1) * 4 + 15) & ~15;
 constexpr int D_SMEM_USED = OFF_SCR + D_EPI_WARPS * 32 * D_SCR_STRIDE * 4;
 // requested: more than a third of the SM's shared memory, so at most two CTAs
 // share an SM and their 2 x 256 tensor-memory columns always fit its 512
 constexpr int D_SMEM = 106 * 1024;
-static_assert(OFF_CNT % 16 == 0, "counter alignment");
+static_assert(OFF_B % 16 == 0 && OFF_CNT % 16 == 0 && OFF_SCR % 16 == 0, "alignment");
 static_assert(D_SMEM_USED <= D_SMEM, "shared memory layout");
 static_assert(3 * (D_SMEM + 2048) > 228 * 1024, "at most two CTAs per SM");
 
@@ -101,7 +111,7 @@ __host__ __device__ constexpr uint32_t make_idesc()
            | ((uint32_t)(DM >> 4) << 24); // M / 16
 }
 
-__device__ __forceinline__ uint32_t core_offset(int r, int chunk16, int rows)
+__host__ __device__ __forceinline__ uint32_t core_offset(int r, int chunk16, int rows)
 {
     // byte offset of the 16-byte chunk chunk16 (0..3) of row r
     return (uint32_t)((chunk16 >> 1) * rows * 32 + (r >> 3) * 256 + (chunk16 & 1) * 128 + (r & 7) * 16);
@@ -109,19 +119,16 @@ __device__ __forceinline__ uint32_t core_offset(int r, int chunk16, int rows)
 
 // one-hot of a packed window, 16 bytes per chunk, with `bias` in byte 63
 // (l <= 15 leaves bytes 60..63 free).  PAD or a missing window: all zero.
-__device__ __forceinline__ void onehot_row(uint8_t *base, int r, int rows, uint32_t w, int l, uint32_t bias)
+__device__ __forceinline__ uint4 onehot_chunk(uint32_t w, int l, uint32_t bias, int c)
 {
+    uint32_t word[4];
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-        uint32_t word[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int pos = 4 * c + q;
-            word[q] = (w != GKM_PAD && pos < l) ? (1u << (8 * ((w >> (2 * pos)) & 3u))) : 0u;
-        }
-        if (c == 3 && w != GKM_PAD) word[3] |= bias << 24;
-        *(uint4 *)(base + core_offset(r, c, rows)) = make_uint4(word[0], word[1], word[2], word[3]);
+    for (int q = 0; q < 4; q++) {
+        const int pos = 4 * c + q;
+        word[q] = (w != GKM_PAD && pos < l) ? (1u << (8 * ((w >> (2 * pos)) & 3u))) : 0u;
     }
+    if (c == 3 && w != GKM_PAD) word[3] |= bias << 24;
+    return make_uint4(word[0], word[1], word[2], word[3]);
 }
 
 __device__ __forceinline__ uint64_t global_ns()
@@ -188,38 +195,88 @@ struct DenseArgs {
     const int32_t *cy;
     int64_t S;
     int64_t Wy;
+    int64_t chunk0;        // first SV chunk of this launch round
+    int64_t max_tiles;     // record slots per chunk
+    const uint8_t *rec;    // [chunks of the round][max_tiles] B records
     double *raw;
     uint64_t *profile;
     int *error;
 };
 
+// chunk-local windows of SV chunk `cg`: prefix counts pre[0..n] (n SVs)
+__device__ __forceinline__ int chunk_prefix(const DenseArgs &a, int64_t cg, int *pre)
+{
+    const int64_t s_lo = cg * D_CH;
+    const int n = (int)min((int64_t)D_CH, a.S - s_lo);
+    const int mult = (a.spec.include_rc && a.ry) ? 2 : 1;
+    pre[0] = 0;
+    for (int s = 0; s < n; s++) pre[s + 1] = pre[s] + mult * a.cy[s_lo + s];
+    return n;
+}
+
+// B records: block (tile i, chunk of the round), thread = column
+__global__ void __launch_bounds__(DN) dense_b_records(DenseArgs a, uint8_t *rec)
+{
+    __shared__ int pre[D_CH + 1];
+    __shared__ int nsv;
+    const int64_t cl = blockIdx.y, cg = a.chunk0 + cl;
+    if (threadIdx.x == 0) nsv = chunk_prefix(a, cg, pre);
+    __syncthreads();
+    const int ny_total = pre[nsv];
+    const int i = blockIdx.x;
+    if ((int64_t)i * DN >= ny_total) return;  // past this chunk's last tile
+    const gkm_spec &sp = a.spec;
+    const uint32_t bias_b = 32u - (uint32_t)(sp.l - sp.dmax);
+    const int j = threadIdx.x, t = i * DN + j;
+    uint32_t w = GKM_PAD;
+    int s = 0;
+    uint8_t wt = 0;
+    if (t < ny_total) {
+        while (t >= pre[s + 1]) s++;
+        const int u = t - pre[s];
+        const int64_t sg = cg * D_CH + s;
+        const int ny = a.cy[sg];
+        if (u < ny) {
+            w = a.by[sg * a.Wy + u];
+            wt = sp.weighted ? (uint8_t)gkm_wt(sp.wd, ny, u) : 1;
+        } else {  // RC of forward window ny - 1 - (u - ny)
+            const int f = ny - 1 - (u - ny);
+            w = a.ry[sg * a.Wy + (a.Wy - 1 - f)];
+            wt = sp.weighted ? (uint8_t)gkm_wt(sp.wd, ny, f) : 1;
+        }
+    }
+    uint8_t *r = rec + (cl * a.max_tiles + i) * (int64_t)REC;
+#pragma unroll
+    for (int c = 0; c < 4; c++) *(uint4 *)(r + core_offset(j, c, DN)) = onehot_chunk(w, sp.l, bias_b, c);
+    r[B_TILE + j] = (uint8_t)s;
+    r[B_TILE + DN + j] = wt;
+}
+
+template <bool C32>
 __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
 {
     extern __shared__ __align__(1024) uint8_t sm[];
     uint8_t *smA = sm + OFF_A;                 // [D_SEG / DM] A tiles, core-matrix layout
-    uint8_t *smB = sm + OFF_B;                 // [2] B tiles
-    uint8_t *col_sv = sm + OFF_COLSV;          // [2][DN] chunk-local SV of each B column
-    uint8_t *col_w = sm + OFF_COLW;            // [2][DN] its window weight
+    uint8_t *smB = sm + OFF_B;                 // [2] B records
     unsigned long long *cnt = (unsigned long long *)(sm + OFF_CNT);  // [D_CH][D_LEVELS]
-    int *pre = (int *)(sm + OFF_PRE);          // [D_CH + 1] window offsets of the chunk's SVs
+    unsigned *cnt32 = (unsigned *)(sm + OFF_CNT);                     // the same, 32-bit
     uint32_t *scratch = (uint32_t *)(sm + OFF_SCR);  // [epilogue warp][lane][D_SCR_STRIDE]
     __shared__ __align__(8) uint64_t bars[N_BARS];
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
+    __shared__ int pre[D_CH + 1];
+    __shared__ int nsv_s;
     volatile int *abort = &abort_flag;
 
     const gkm_spec &sp = a.spec;
     const int l = sp.l, dmax = sp.dmax;
     // a pair's accumulator is matches + bias_b (byte 63 of A is 1, of B is
-    // bias_b): at least 32 -- bit 5 set -- exactly when it has at least l - dmax
-    // matches, and below 48 since matches <= l <= 15.  Pairs with a PAD
-    // window or a missing column accumulate 0.
-    const uint32_t bias_b = 32u - (uint32_t)(l - dmax);
+    // bias_b = 32 - (l - dmax)): at least 32 -- bit 5 set -- exactly when it
+    // has at least l - dmax matches, and below 48 since matches <= l <= 15.
+    // Pairs with a PAD window or a missing column accumulate 0.
     const int64_t b = blockIdx.x;
-    const int64_t s_lo = (int64_t)blockIdx.y * D_CH;
-    const int nsv = (int)min((int64_t)D_CH, a.S - s_lo);
+    const int64_t cl = blockIdx.y, cg = a.chunk0 + cl;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const bool has_rc = sp.include_rc && a.ry != nullptr;
     const uint32_t bar0 = smem_addr(bars);
     auto bar = [&](int k) { return bar0 + 8u * (uint32_t)k; };
 
@@ -232,12 +289,11 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
 
     for (int k = tid; k < D_CH * D_LEVELS; k += D_THREADS) cnt[k] = 0;
     if (tid == 0) {
-        pre[0] = 0;
-        for (int s = 0; s < nsv; s++) pre[s + 1] = pre[s] + (has_rc ? 2 : 1) * a.cy[s_lo + s];
-        // B buffers: filled by each producer warp, emptied by every epilogue
+        nsv_s = chunk_prefix(a, cg, pre);
+        // B buffers: filled by the producer's copy, emptied by every epilogue
         // warp; accumulators: filled by the MMA commit, emptied by the four
         // warps of their warpgroup
-        const uint32_t counts[N_BARS] = {D_PROD_WARPS, D_PROD_WARPS, D_EPI_WARPS, D_EPI_WARPS, 1, 1, 4, 4, 1};
+        const uint32_t counts[N_BARS] = {1, 1, D_EPI_WARPS, D_EPI_WARPS, 1, 1, 4, 4, 1};
         for (int k = 0; k < N_BARS; k++)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar(k)), "r"(counts[k]));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -251,11 +307,13 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
-    const int ny_total = pre[nsv];
-    const int NB = (ny_total + DN - 1) / DN;
+    const int nsv = nsv_s;
+    const int NB = (pre[nsv] + DN - 1) / DN;
     const int nx = a.cx[b];
     const uint32_t idesc = make_idesc();
+    const uint8_t *rec = a.rec + cl * a.max_tiles * (int64_t)REC;
     uint32_t g_base = 0, t_base = 0;  // B tiles and tile pairs of earlier segments
+    uint32_t copies = 0;              // B records the producer has requested
 
     for (int seg0 = 0; seg0 < nx && NB > 0; seg0 += D_SEG) {
         const int nseg = min(D_SEG, nx - seg0);
@@ -263,7 +321,9 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
         // every warp: this segment's A tiles (rows past the row's end: zero)
         for (int r = tid; r < NA * DM; r += D_THREADS) {
             const uint32_t w = r < nseg ? a.bx[b * a.Wx + seg0 + r] : GKM_PAD;
-            onehot_row(smA + (r / DM) * A_TILE, r % DM, DM, w, l, 1u);
+            uint8_t *base = smA + (r / DM) * A_TILE;
+#pragma unroll
+            for (int c = 0; c < 4; c++) *(uint4 *)(base + core_offset(r % DM, c, DM)) = onehot_chunk(w, l, 1u, c);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -276,8 +336,8 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
             uint32_t *scr = scratch + warp * 32 * D_SCR_STRIDE;
             for (int bt = 0; bt < NB; bt++) {
                 const uint32_t g = g_base + bt, buf = g & 1u;
-                const uint8_t *csv = col_sv + buf * DN, *cw = col_w + buf * DN;
-                // wait for this B tile to be filled even when none of its tiles is
+                const uint8_t *csv = smB + buf * REC + B_TILE, *cw = csv + DN;
+                // wait for this B tile to land even when none of its tiles is
                 // ours: the release below must not count toward an earlier
                 // phase of the buffer while the other warpgroup still reads it
                 bool ok = __all_sync(GKM_FULL, bar_wait(bar(BAR_BFULL + buf), (g >> 1) & 1u, abort, a.error));
@@ -320,16 +380,19 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
                         }
                         __syncwarp();
                         const int col = 32 * k + lane;
-                        const uint32_t csv_l = csv[col], cw_l = cw[col];
+                        const uint32_t base = (uint32_t)csv[col] * D_LEVELS + 32 + dmax, cw_l = cw[col];
                         while (rows) {
                             const int q = __ffs(rows) - 1;
                             rows &= rows - 1;
                             const uint32_t word = scr[q * D_SCR_STRIDE + (lane >> 1)];
                             const uint32_t v = (lane & 1) ? (word >> 16) : (word & 0xFFFFu);
-                            const uint32_t wq = __shfl_sync(GKM_FULL, wx, q);
-                            if (v & 32u)  // mismatches l - (v - bias_b)
-                                atomicAdd(&cnt[csv_l * D_LEVELS + (32 + dmax - (int)v)],
-                                          (unsigned long long)(wq * cw_l));
+                            if (C32) {  // unweighted: every pair counts 1
+                                if (v & 32u) atomicAdd(cnt32 + (base - v), 1u);
+                            } else {
+                                const uint32_t wq = __shfl_sync(GKM_FULL, wx, q);
+                                if (v & 32u)  // mismatches l - (v - bias_b)
+                                    atomicAdd(cnt + (base - v), (unsigned long long)(wq * cw_l));
+                            }
                         }
                         __syncwarp();  // scratch is rewritten by the next chunk
                     }
@@ -338,44 +401,22 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
                 __syncwarp();  // B tile's column tables no longer read: hand the buffer back
                 if (lane == 0) bar_arrive(bar(BAR_BEMPTY + buf));
             }
-        } else if (warp < D_MMA_WARP) {
-            // ---- producers: B tiles, DN columns each
-            const int pl = tid - D_EPI_WARPS * 32;  // 0 .. D_PROD_WARPS * 32 - 1
-            for (int bt = 0; bt < NB; bt++) {
-                const uint32_t g = g_base + bt, buf = g & 1u;
-                if (g >= 2) {
-                    // each producer warp waits and decides alone (no barrier
-                    // joins the two warps, so one leaving never blocks the other)
-                    const bool ok = bar_wait(bar(BAR_BEMPTY + buf), ((g >> 1) - 1) & 1u, abort, a.error);
-                    if (!__all_sync(GKM_FULL, ok)) break;
+        } else if (warp == D_PROD_WARP) {
+            // ---- producer: one bulk copy per B record
+            if (lane == 0) {
+                for (int bt = 0; bt < NB; bt++) {
+                    const uint32_t g = g_base + bt, buf = g & 1u;
+                    if (g >= 2 && !bar_wait(bar(BAR_BEMPTY + buf), ((g >> 1) - 1) & 1u, abort, a.error)) break;
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar(BAR_BFULL + buf)),
+                                 "r"((uint32_t)REC)
+                                 : "memory");
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                            smem_addr(smB + buf * REC)),
+                        "l"(rec + (int64_t)bt * REC), "r"((uint32_t)REC), "r"(bar(BAR_BFULL + buf))
+                        : "memory");
+                    copies = g + 1;
                 }
-                for (int j = pl; j < DN; j += D_PROD_WARPS * 32) {
-                    const int t = bt * DN + j;
-                    uint32_t w = GKM_PAD;
-                    int s = 0;
-                    uint8_t wt = 0;
-                    if (t < ny_total) {
-                        while (t >= pre[s + 1]) s++;
-                        const int u = t - pre[s];
-                        const int64_t sg = s_lo + s;
-                        const int ny = a.cy[sg];
-                        if (u < ny) {
-                            w = a.by[sg * a.Wy + u];
-                            wt = sp.weighted ? (uint8_t)gkm_wt(sp.wd, ny, u) : 1;
-                        } else {  // RC of forward window ny - 1 - (u - ny)
-                            const int f = ny - 1 - (u - ny);
-                            w = a.ry[sg * a.Wy + (a.Wy - 1 - f)];
-                            wt = sp.weighted ? (uint8_t)gkm_wt(sp.wd, ny, f) : 1;
-                        }
-                    }
-                    onehot_row(smB + buf * B_TILE, j, DN, w, l, bias_b);
-                    col_sv[buf * DN + j] = (uint8_t)s;
-                    col_w[buf * DN + j] = wt;
-                }
-                // this warp's columns are written: one arrival per producer warp
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) bar_arrive(bar(BAR_BFULL + buf));
             }
         } else if (lane == 0) {
             // ---- MMA issue: every (B tile, A tile) pair, accumulators alternating
@@ -391,7 +432,7 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
 #pragma unroll
                     for (int kb = 0; kb < 2; kb++) {
                         const uint64_t da = make_sdesc(smem_addr(smA + at * A_TILE) + kb * DM * 32, 128, 256);
-                        const uint64_t db = make_sdesc(smem_addr(smB + buf * B_TILE) + kb * DN * 32, 128, 256);
+                        const uint64_t db = make_sdesc(smem_addr(smB + buf * REC) + kb * DN * 32, 128, 256);
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
                             "setp.ne.b32 p, %4, 0;\n\t"
@@ -408,6 +449,14 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
         __syncthreads();  // segment done (or abandoned): A is restaged next
         if (abort_flag) break;
     }
+    if (abort_flag && warp == D_PROD_WARP && lane == 0) {
+        // copies in flight land in the B buffers: wait for the last one of
+        // each buffer (bounded) before the block's shared memory is released
+        for (uint32_t g = copies > 2 ? copies - 2 : 0; g < copies; g++) {
+            int ignore = 0;
+            bar_wait(bar(BAR_BFULL + (g & 1u)), (g >> 1) & 1u, &ignore, a.error);
+        }
+    }
     // every MMA issued has completed before its accumulator columns are
     // released (bounded: on a stuck MMA the wait runs out and the error is set)
     if (warp == D_MMA_WARP && lane == 0) {
@@ -421,12 +470,15 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(D_TMEM_COLS));
     if (abort_flag) return;
     for (int s = tid; s < nsv; s += D_THREADS) {
-        const int64_t sg = s_lo + s;
+        const int64_t sg = cg * D_CH + s;
+        auto count = [&](int m) -> uint64_t {
+            return C32 ? (uint64_t)cnt32[s * D_LEVELS + m] : (uint64_t)cnt[s * D_LEVELS + m];
+        };
         double k = 0.0;
-        for (int m = 0; m <= dmax; m++) k += sp.h[m] * (double)cnt[s * D_LEVELS + m];
+        for (int m = 0; m <= dmax; m++) k += sp.h[m] * (double)count(m);
         if (a.raw) a.raw[b * a.S + sg] = k;
         if (a.profile)
-            for (int m = 0; m <= l; m++) a.profile[(b * a.S + sg) * (l + 1) + m] = m <= dmax ? cnt[s * D_LEVELS + m] : 0;
+            for (int m = 0; m <= l; m++) a.profile[(b * a.S + sg) * (l + 1) + m] = m <= dmax ? count(m) : 0;
     }
 }
 
@@ -443,9 +495,22 @@ extern "C" int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, cons
     if (spec->weighted && (!spec->wd || spec->wd_len < 1)) return gkm_fail(GKM_ERR_INVALID, "weighted spec without weights");
     if (B == 0 || S == 0) return GKM_OK;
     if (!bx || !cx || !by || !cy || !error) return gkm_fail(GKM_ERR_INVALID, "null argument");
-    if (B > 0x7FFFFFFFLL || (S + D_CH - 1) / D_CH > 65535)
-        return gkm_fail(GKM_ERR_UNSUPPORTED, "too many rows or columns for one dense launch");
+    if (B > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many rows for one dense launch");
     if ((int64_t)D_CH * 2 * Wy > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "columns too long for one dense launch");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int mult = (spec->include_rc && ry) ? 2 : 1;
+    const int64_t chunks = (S + D_CH - 1) / D_CH;
+    const int64_t max_tiles = (D_CH * mult * Wy + DN - 1) / DN;
+    const size_t per_chunk = (size_t)max_tiles * REC;
+    int64_t round = (int64_t)(D_REC_BUDGET / per_chunk);
+    if (round < 1) round = 1;
+    if (round > chunks) round = chunks;
+    if (round > 65535) round = 65535;
+    uint8_t *rec = nullptr;
+    if (cudaMallocAsync(&rec, per_chunk * round, st) != cudaSuccess) return gkm_fail(GKM_ERR_OOM, "dense B records");
+    // 32-bit counters when no count can reach 2^32: unweighted, and at most
+    // Wx x (mult Wy) pairs of one (row, SV)
+    const bool c32 = !spec->weighted && (int64_t)Wx * mult * Wy < 0xFFFFFFFFLL;
     DenseArgs a;
     a.spec = *spec;
     a.bx = bx;
@@ -456,12 +521,29 @@ extern "C" int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, cons
     a.cy = cy;
     a.S = S;
     a.Wy = Wy;
+    a.max_tiles = max_tiles;
+    a.rec = rec;
     a.raw = raw;
     a.profile = profile;
     a.error = error;
-    cudaFuncSetAttribute(dense_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, D_SMEM);
-    dim3 grid((unsigned)B, (unsigned)((S + D_CH - 1) / D_CH));
-    dense_pairs_kernel<<<grid, D_THREADS, D_SMEM, (cudaStream_t)stream>>>(a);
-    GKM_CHECK_LAUNCH("dense_pairs");
-    return GKM_OK;
+    if (c32) cudaFuncSetAttribute(dense_pairs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, D_SMEM);
+    else cudaFuncSetAttribute(dense_pairs_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, D_SMEM);
+    int s = GKM_OK;
+    for (int64_t c0 = 0; c0 < chunks && s == GKM_OK; c0 += round) {
+        const int64_t nc = chunks - c0 < round ? chunks - c0 : round;
+        a.chunk0 = c0;
+        dense_b_records<<<dim3((unsigned)max_tiles, (unsigned)nc), DN, 0, st>>>(a, rec);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            s = gkm_cuda_status(e, "dense_b_records");
+            break;
+        }
+        const dim3 grid((unsigned)B, (unsigned)nc);
+        if (c32) dense_pairs_kernel<true><<<grid, D_THREADS, D_SMEM, st>>>(a);
+        else dense_pairs_kernel<false><<<grid, D_THREADS, D_SMEM, st>>>(a);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) s = gkm_cuda_status(e, "dense_pairs");
+    }
+    cudaFreeAsync(rec, st);
+    return s;
 }

@@ -111,30 +111,21 @@ def dense_pairwise(spec: Spec, bx, cx, by, ry, cy, raw: bool = True, profile: bo
 
 
 # Pairwise method: "join" (warp ballot/popc over window pairs), "dense"
-# (tensor-core one-hot product), or "auto".  The tensor-core product costs the
-# same per window pair whatever dmax is, but every pair within dmax (a "hit")
-# then goes through a shared-memory counter, so it wins where hits are rare:
-# auto picks dense where it applies, the query rows have at least
-# DENSE_MIN_WINDOWS windows (shorter rows leave most of a 128-row tile empty)
-# and a random pair of l-mers is within dmax with probability at most
-# DENSE_MAX_HIT_RATE (measured crossover on B200: about 5e-3; l = 11, dmax = 3
-# is 1.2e-3 and runs 2.4x the join).
+# (tensor-core one-hot product), or "auto": the tensor-core product wherever
+# it applies (0 <= dmax < l <= 15).  Measured on B200 it runs 1.2x (60 bp
+# rows) to 4x (long rows, or dmax = 10) the join's window pairs per second.
 PAIRWISE_METHOD = "auto"
-DENSE_MIN_WINDOWS = 128
-DENSE_MAX_HIT_RATE = 4e-3
 
 
 def hit_rate(l: int, dmax: int) -> float:
-    """Probability that two uniform random l-mers differ at <= dmax positions."""
+    """Probability that two uniform random l-mers differ at <= dmax positions
+    (the share of window pairs the dense epilogue counts)."""
     from math import comb
     return sum(comb(l, m) * 0.75 ** m * 0.25 ** (l - m) for m in range(dmax + 1))
 
 
 def choose_pairwise(spec: Spec, Wx: int) -> str:
-    b = spec.base
-    if dense_applies(spec) and Wx >= DENSE_MIN_WINDOWS and hit_rate(b.l, b.dmax) <= DENSE_MAX_HIT_RATE:
-        return "dense"
-    return "join"
+    return "dense" if dense_applies(spec) else "join"
 
 
 def pairwise(spec: Spec, bx, cx, by, ry, cy, raw: bool = True, profile: bool = False, method: str | None = None):

@@ -140,7 +140,7 @@ def test_abi_library_exports_every_declared_symbol():
 
 
 def test_pairwise_dispatch_rule():
-    """auto picks the tensor-core product only where hits are rare and rows long."""
+    """auto takes the tensor-core product wherever it applies (dmax < l <= 15)."""
     import torch
 
     from gkmsvm_lite_b200 import engine
@@ -149,13 +149,10 @@ def test_pairwise_dispatch_rule():
         m = gk.GkmSVM(np.zeros((2, 40), np.uint8), np.ones(2), 0.0, kt, p)
         return engine.Spec(m.kernel.base, torch.device("cpu"))
 
-    # exact: l-mers within 3 of a given one, over all 4^11
     from math import comb
+    # exact: l-mers within 3 of a given one, over all 4^11
     want = sum(comb(11, m) * 3 ** m for m in range(4)) / 4 ** 11
     assert abs(engine.hit_rate(11, 3) - want) < 1e-15
-    d = spec("gkm_esttrunc", dict(L=11, k=7, d=3))
-    assert engine.choose_pairwise(d, 990) == "dense"
-    assert engine.choose_pairwise(d, 50) == "join"  # short rows
-    assert engine.choose_pairwise(spec("gkm_cnt", dict(L=11, k=7)), 990) == "join"  # dmax 4: hits too common
-    assert engine.choose_pairwise(spec("gkm_cnt", dict(L=15, k=5, d=10)), 990) == "join"
+    assert engine.choose_pairwise(spec("gkm_esttrunc", dict(L=11, k=7, d=3)), 50) == "dense"
+    assert engine.choose_pairwise(spec("gkm_cnt", dict(L=15, k=5, d=10)), 990) == "dense"
     assert engine.choose_pairwise(spec("wgkm", dict(L=9, k=6, d=2)), 990) == "dense"
