@@ -19,10 +19,11 @@
 //                    SV -- are packed into consecutive tiles across SV
 //                    boundaries.
 //   dense_pairs_kernel  one CTA per (query row, SV chunk), with warp roles:
-//     - all warps first stage the row's one-hot (up to D_SEG windows: 8 A
-//       tiles) in shared memory, where it stays;
+//     - all warps first stage a segment of the row's one-hot (up to 1,024
+//       windows: 8 A tiles; 512 for weighted kernels) in shared memory, where
+//       it stays while every B tile of the chunk passes;
 //     - one producer thread copies the chunk's B records, one per tile, into a
-//       double buffer with cp.async.bulk (untiled, 16-byte aligned, a multiple
+//       ring of 3 (4 weighted) buffers with cp.async.bulk (untiled, 16-byte aligned, a multiple
 //       of 16 bytes, completing on the buffer's mbarrier);
 //     - one thread issues the MMAs of every (B tile, A tile) pair, alternating
 //       between two accumulators in tensor memory, and commits each to an
@@ -32,8 +33,8 @@
 //       straight back to the MMA thread, and only then look for pairs within
 //       dmax: an OR over each 32-column chunk and a warp ballot; the rare rows
 //       with a hit leave their values in shared scratch and the warp walks
-//       them one row at a time, a column per lane, into shared per-(SV, level)
-//       counters (32-bit where the launch's totals fit, else 64-bit).
+//       them one row at a time, a column per lane, into per-(SV, level)
+//       counters (see the counting modes below).
 // mbarriers hand buffers between the roles (full/empty pairs); every wait is
 // bounded in time and raises the launch's error flag when it runs out, after
 // which every role leaves its loop, the MMA thread waits (bounded) for its
@@ -55,7 +56,6 @@ namespace {
 constexpr int DM = 128;            // query windows per A tile (MMA M)
 constexpr int DN = 128;            // SV windows per B tile (MMA N)
 constexpr int DKB = 64;            // one-hot bytes per window
-constexpr int D_SEG = 1024;        // query windows staged at a time (8 A tiles)
 constexpr int D_CH = 16;           // SVs per chunk (per CTA)
 constexpr int D_LEVELS = 16;
 constexpr int D_EPI_WARPS = 8;     // warps 0..7: warpgroup w / 4 drains accumulator w / 4,
@@ -71,22 +71,50 @@ constexpr uint64_t D_WAIT_NS = 1000000000ull;  // give up on a hand-off after 1 
 constexpr size_t D_REC_BUDGET = (size_t)1 << 30;  // B records per launch round
 static_assert(REC % 16 == 0, "bulk copies move multiples of 16 bytes");
 
-// dynamic shared memory
-constexpr int OFF_A = 0;
-constexpr int OFF_B = OFF_A + D_SEG * DKB;
-constexpr int OFF_CNT = OFF_B + 2 * REC;
-constexpr int OFF_SCR = OFF_CNT + D_CH * D_LEVELS * 8;
-constexpr int D_SCR_STRIDE = 20;   // words per lane (16 used; 20 keeps 16-byte stores conflict-free)
-constexpr int D_SMEM_USED = OFF_SCR + D_EPI_WARPS * 32 * D_SCR_STRIDE * 4;
-// requested: more than a third of the SM's shared memory, so at most two CTAs
-// share an SM and their 2 x 256 tensor-memory columns always fit its 512
-constexpr int D_SMEM = 106 * 1024;
-static_assert(OFF_B % 16 == 0 && OFF_CNT % 16 == 0 && OFF_SCR % 16 == 0, "alignment");
-static_assert(D_SMEM_USED <= D_SMEM, "shared memory layout");
-static_assert(3 * (D_SMEM + 2048) > 228 * 1024, "at most two CTAs per SM");
+// Counting modes: unweighted launches count each pair 1 in the block's shared
+// counters, 32-bit when no (row, SV) can reach 2^32 pairs, else 64-bit;
+// weighted launches count pair weights (up to 255 x 255) in per-warp 32-bit
+// counters flushed into the block's 64-bit counters before they could wrap.
+enum { MODE_U32 = 0, MODE_U64 = 1, MODE_WEIGHTED = 2 };
+constexpr int D_BBUF_MAX = 4;
+constexpr int D_SCR_STRIDE = 20;   // scratch words per lane (16 used; 20 keeps 16-byte stores conflict-free)
+
+// Shared-memory layout of a mode: staged query segment (A tiles), ring of B
+// records, block counters, per-warp counters (weighted), hit scratch.  Each
+// fits two CTAs per SM and requests more than a third of the SM's shared
+// memory, so at most two CTAs share an SM and their 2 x 256 tensor-memory
+// columns always fit its 512.
+template <int MODE>
+struct Cfg {
+    static constexpr bool weighted = MODE == MODE_WEIGHTED;
+    static constexpr int SEG = weighted ? 512 : 1024;  // query windows staged at a time
+    static constexpr int BBUF = weighted ? 4 : 3;      // B records in flight
+    static constexpr int OFF_A = 0;
+    static constexpr int OFF_B = OFF_A + SEG * DKB;
+    static constexpr int OFF_CNT = OFF_B + BBUF * REC;
+    static constexpr int OFF_WCNT = OFF_CNT + D_CH * D_LEVELS * 8;
+    static constexpr int OFF_SCR = OFF_WCNT + (weighted ? D_EPI_WARPS * D_CH * D_LEVELS * 4 : 0);
+    static constexpr int USED = OFF_SCR + D_EPI_WARPS * 32 * D_SCR_STRIDE * 4;
+    static constexpr int SMEM = ((USED + 1023) / 1024) * 1024;
+    // a warp's counters gain at most its 32 rows x 128 columns of each of its
+    // warpgroup's A tiles of one B tile, times the largest pair weight
+    static constexpr uint64_t WARP_PAIRS_PER_B = 32ull * DN * (SEG / DM / 2);
+    static_assert(OFF_B % 16 == 0 && OFF_CNT % 16 == 0 && OFF_WCNT % 16 == 0 && OFF_SCR % 16 == 0, "alignment");
+    static_assert(BBUF <= D_BBUF_MAX, "barrier slots");
+    static_assert(2 * (SMEM + 2048) <= 228 * 1024, "two CTAs per SM");
+    static_assert(3 * (SMEM + 1024) > 228 * 1024, "at most two CTAs per SM");
+    static_assert(WARP_PAIRS_PER_B * 255 * 255 < (1ull << 32), "per-warp counters cannot wrap");
+};
 
 // mbarriers (static shared memory)
-enum { BAR_BFULL = 0, BAR_BEMPTY = 2, BAR_TFULL = 4, BAR_TEMPTY = 6, BAR_DONE = 8, N_BARS = 9 };
+enum {
+    BAR_BFULL = 0,
+    BAR_BEMPTY = BAR_BFULL + D_BBUF_MAX,
+    BAR_TFULL = BAR_BEMPTY + D_BBUF_MAX,
+    BAR_TEMPTY = BAR_TFULL + 2,
+    BAR_DONE = BAR_TEMPTY + 2,
+    N_BARS = BAR_DONE + 1
+};
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -197,6 +225,7 @@ struct DenseArgs {
     int64_t Wy;
     int64_t chunk0;        // first SV chunk of this launch round
     int64_t max_tiles;     // record slots per chunk
+    int flush_every;       // B tiles between flushes of the per-warp counters
     const uint8_t *rec;    // [chunks of the round][max_tiles] B records
     double *raw;
     uint64_t *profile;
@@ -252,15 +281,19 @@ __global__ void __launch_bounds__(DN) dense_b_records(DenseArgs a, uint8_t *rec)
     r[B_TILE + DN + j] = wt;
 }
 
-template <bool C32>
+template <int MODE>
 __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
 {
+    using C = Cfg<MODE>;
+    constexpr bool WEIGHTED = C::weighted;
+    constexpr int D_SEG = C::SEG, D_BBUF = C::BBUF;
     extern __shared__ __align__(1024) uint8_t sm[];
-    uint8_t *smA = sm + OFF_A;                 // [D_SEG / DM] A tiles, core-matrix layout
-    uint8_t *smB = sm + OFF_B;                 // [2] B records
-    unsigned long long *cnt = (unsigned long long *)(sm + OFF_CNT);  // [D_CH][D_LEVELS]
-    unsigned *cnt32 = (unsigned *)(sm + OFF_CNT);                     // the same, 32-bit
-    uint32_t *scratch = (uint32_t *)(sm + OFF_SCR);  // [epilogue warp][lane][D_SCR_STRIDE]
+    uint8_t *smA = sm + C::OFF_A;              // [D_SEG / DM] A tiles, core-matrix layout
+    uint8_t *smB = sm + C::OFF_B;              // [D_BBUF] B records
+    unsigned long long *cnt = (unsigned long long *)(sm + C::OFF_CNT);  // [D_CH][D_LEVELS]
+    unsigned *cnt32 = (unsigned *)(sm + C::OFF_CNT);                     // the same, 32-bit (MODE_U32)
+    unsigned *wcnt_all = (unsigned *)(sm + C::OFF_WCNT);  // [epilogue warp][D_CH][D_LEVELS] (weighted)
+    uint32_t *scratch = (uint32_t *)(sm + C::OFF_SCR);    // [epilogue warp][lane][D_SCR_STRIDE]
     __shared__ __align__(8) uint64_t bars[N_BARS];
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
@@ -288,14 +321,18 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
     if (abort_flag) return;
 
     for (int k = tid; k < D_CH * D_LEVELS; k += D_THREADS) cnt[k] = 0;
+    if (WEIGHTED)
+        for (int k = tid; k < D_EPI_WARPS * D_CH * D_LEVELS; k += D_THREADS) wcnt_all[k] = 0;
     if (tid == 0) {
         nsv_s = chunk_prefix(a, cg, pre);
         // B buffers: filled by the producer's copy, emptied by every epilogue
         // warp; accumulators: filled by the MMA commit, emptied by the four
         // warps of their warpgroup
-        const uint32_t counts[N_BARS] = {1, 1, D_EPI_WARPS, D_EPI_WARPS, 1, 1, 4, 4, 1};
-        for (int k = 0; k < N_BARS; k++)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar(k)), "r"(counts[k]));
+        for (int k = 0; k < N_BARS; k++) {
+            const uint32_t n = k < BAR_BEMPTY ? 1 : k < BAR_TFULL ? D_EPI_WARPS : k < BAR_TEMPTY ? 1
+                             : k < BAR_DONE ? 4 : 1;
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar(k)), "r"(n));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -334,13 +371,14 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
             const uint32_t eg = (uint32_t)(warp >> 2);
             const int quad = warp & 3;
             uint32_t *scr = scratch + warp * 32 * D_SCR_STRIDE;
+            unsigned *wcnt = wcnt_all + warp * D_CH * D_LEVELS;
             for (int bt = 0; bt < NB; bt++) {
-                const uint32_t g = g_base + bt, buf = g & 1u;
+                const uint32_t g = g_base + bt, buf = g % D_BBUF;
                 const uint8_t *csv = smB + buf * REC + B_TILE, *cw = csv + DN;
                 // wait for this B tile to land even when none of its tiles is
                 // ours: the release below must not count toward an earlier
                 // phase of the buffer while the other warpgroup still reads it
-                bool ok = __all_sync(GKM_FULL, bar_wait(bar(BAR_BFULL + buf), (g >> 1) & 1u, abort, a.error));
+                bool ok = __all_sync(GKM_FULL, bar_wait(bar(BAR_BFULL + buf), (g / D_BBUF) & 1u, abort, a.error));
                 if (!ok) break;
                 for (int at = 0; at < NA; at++) {
                     const uint32_t t = t_base + (uint32_t)(bt * NA + at), slot = t & 1u;
@@ -386,12 +424,14 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
                             rows &= rows - 1;
                             const uint32_t word = scr[q * D_SCR_STRIDE + (lane >> 1)];
                             const uint32_t v = (lane & 1) ? (word >> 16) : (word & 0xFFFFu);
-                            if (C32) {  // unweighted: every pair counts 1
-                                if (v & 32u) atomicAdd(cnt32 + (base - v), 1u);
-                            } else {
+                            // mismatches l - (v - bias_b)
+                            if (MODE == MODE_WEIGHTED) {
                                 const uint32_t wq = __shfl_sync(GKM_FULL, wx, q);
-                                if (v & 32u)  // mismatches l - (v - bias_b)
-                                    atomicAdd(cnt + (base - v), (unsigned long long)(wq * cw_l));
+                                if (v & 32u) atomicAdd(wcnt + (base - v), wq * cw_l);
+                            } else if (MODE == MODE_U32) {
+                                if (v & 32u) atomicAdd(cnt32 + (base - v), 1u);
+                            } else if (v & 32u) {
+                                atomicAdd(cnt + (base - v), 1ull);
                             }
                         }
                         __syncwarp();  // scratch is rewritten by the next chunk
@@ -400,13 +440,24 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
                 if (!ok) break;
                 __syncwarp();  // B tile's column tables no longer read: hand the buffer back
                 if (lane == 0) bar_arrive(bar(BAR_BEMPTY + buf));
+                if (WEIGHTED && ((g + 1) % (uint32_t)a.flush_every == 0 || bt + 1 == NB)) {
+                    // this warp's counts into the block's 64-bit counters
+                    for (int k = lane; k < D_CH * D_LEVELS; k += 32) {
+                        const unsigned c = wcnt[k];
+                        if (c) {
+                            atomicAdd(cnt + k, (unsigned long long)c);
+                            wcnt[k] = 0;
+                        }
+                    }
+                    __syncwarp();
+                }
             }
         } else if (warp == D_PROD_WARP) {
             // ---- producer: one bulk copy per B record
             if (lane == 0) {
                 for (int bt = 0; bt < NB; bt++) {
-                    const uint32_t g = g_base + bt, buf = g & 1u;
-                    if (g >= 2 && !bar_wait(bar(BAR_BEMPTY + buf), ((g >> 1) - 1) & 1u, abort, a.error)) break;
+                    const uint32_t g = g_base + bt, buf = g % D_BBUF;
+                    if (g >= D_BBUF && !bar_wait(bar(BAR_BEMPTY + buf), (g / D_BBUF - 1) & 1u, abort, a.error)) break;
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar(BAR_BFULL + buf)),
                                  "r"((uint32_t)REC)
                                  : "memory");
@@ -422,8 +473,8 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
             // ---- MMA issue: every (B tile, A tile) pair, accumulators alternating
             bool ok = true;
             for (int bt = 0; bt < NB && ok; bt++) {
-                const uint32_t g = g_base + bt, buf = g & 1u;
-                ok = bar_wait(bar(BAR_BFULL + buf), (g >> 1) & 1u, abort, a.error);
+                const uint32_t g = g_base + bt, buf = g % D_BBUF;
+                ok = bar_wait(bar(BAR_BFULL + buf), (g / D_BBUF) & 1u, abort, a.error);
                 for (int at = 0; at < NA && ok; at++) {
                     const uint32_t t = t_base + (uint32_t)(bt * NA + at), slot = t & 1u;
                     if (t >= 2) ok = bar_wait(bar(BAR_TEMPTY + slot), ((t >> 1) - 1) & 1u, abort, a.error);
@@ -452,9 +503,9 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
     if (abort_flag && warp == D_PROD_WARP && lane == 0) {
         // copies in flight land in the B buffers: wait for the last one of
         // each buffer (bounded) before the block's shared memory is released
-        for (uint32_t g = copies > 2 ? copies - 2 : 0; g < copies; g++) {
+        for (uint32_t g = copies > D_BBUF ? copies - D_BBUF : 0; g < copies; g++) {
             int ignore = 0;
-            bar_wait(bar(BAR_BFULL + (g & 1u)), (g >> 1) & 1u, &ignore, a.error);
+            bar_wait(bar(BAR_BFULL + g % D_BBUF), (g / D_BBUF) & 1u, &ignore, a.error);
         }
     }
     // every MMA issued has completed before its accumulator columns are
@@ -472,7 +523,7 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
     for (int s = tid; s < nsv; s += D_THREADS) {
         const int64_t sg = cg * D_CH + s;
         auto count = [&](int m) -> uint64_t {
-            return C32 ? (uint64_t)cnt32[s * D_LEVELS + m] : (uint64_t)cnt[s * D_LEVELS + m];
+            return MODE == MODE_U32 ? (uint64_t)cnt32[s * D_LEVELS + m] : (uint64_t)cnt[s * D_LEVELS + m];
         };
         double k = 0.0;
         for (int m = 0; m <= dmax; m++) k += sp.h[m] * (double)count(m);
@@ -508,9 +559,9 @@ extern "C" int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, cons
     if (round > 65535) round = 65535;
     uint8_t *rec = nullptr;
     if (cudaMallocAsync(&rec, per_chunk * round, st) != cudaSuccess) return gkm_fail(GKM_ERR_OOM, "dense B records");
-    // 32-bit counters when no count can reach 2^32: unweighted, and at most
-    // Wx x (mult Wy) pairs of one (row, SV)
-    const bool c32 = !spec->weighted && (int64_t)Wx * mult * Wy < 0xFFFFFFFFLL;
+    // 32-bit block counters when no (row, SV) can reach 2^32 unweighted pairs
+    const int mode = spec->weighted ? MODE_WEIGHTED
+                     : (int64_t)Wx * mult * Wy < 0xFFFFFFFFLL ? MODE_U32 : MODE_U64;
     DenseArgs a;
     a.spec = *spec;
     a.bx = bx;
@@ -522,12 +573,17 @@ extern "C" int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, cons
     a.S = S;
     a.Wy = Wy;
     a.max_tiles = max_tiles;
+    a.flush_every = (int)(0xFFFFFFFFull / (Cfg<MODE_WEIGHTED>::WARP_PAIRS_PER_B * 255ull * 255ull));
     a.rec = rec;
     a.raw = raw;
     a.profile = profile;
     a.error = error;
-    if (c32) cudaFuncSetAttribute(dense_pairs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, D_SMEM);
-    else cudaFuncSetAttribute(dense_pairs_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, D_SMEM);
+    cudaFuncSetAttribute(dense_pairs_kernel<MODE_U32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         Cfg<MODE_U32>::SMEM);
+    cudaFuncSetAttribute(dense_pairs_kernel<MODE_U64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         Cfg<MODE_U64>::SMEM);
+    cudaFuncSetAttribute(dense_pairs_kernel<MODE_WEIGHTED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         Cfg<MODE_WEIGHTED>::SMEM);
     int s = GKM_OK;
     for (int64_t c0 = 0; c0 < chunks && s == GKM_OK; c0 += round) {
         const int64_t nc = chunks - c0 < round ? chunks - c0 : round;
@@ -539,8 +595,12 @@ extern "C" int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, cons
             break;
         }
         const dim3 grid((unsigned)B, (unsigned)nc);
-        if (c32) dense_pairs_kernel<true><<<grid, D_THREADS, D_SMEM, st>>>(a);
-        else dense_pairs_kernel<false><<<grid, D_THREADS, D_SMEM, st>>>(a);
+        if (mode == MODE_U32)
+            dense_pairs_kernel<MODE_U32><<<grid, D_THREADS, Cfg<MODE_U32>::SMEM, st>>>(a);
+        else if (mode == MODE_U64)
+            dense_pairs_kernel<MODE_U64><<<grid, D_THREADS, Cfg<MODE_U64>::SMEM, st>>>(a);
+        else
+            dense_pairs_kernel<MODE_WEIGHTED><<<grid, D_THREADS, Cfg<MODE_WEIGHTED>::SMEM, st>>>(a);
         e = cudaGetLastError();
         if (e != cudaSuccess) s = gkm_cuda_status(e, "dense_pairs");
     }
