@@ -443,8 +443,10 @@ def run_b200(args):
     result = None
     if rank == 0:
         # roofline of the dominant kernel: the fused index query (algorithmic
-        # bytes: lookups x 8 B + hits x 4 B + 12 B per query window; hits
-        # counted exactly on the first queries and scaled by windows)
+        # bytes: lookups x 8 B (a bucket's two offsets) + hits x the stored
+        # entry size (2 B: SV ids within a tile of <= 65,536 SVs, unweighted)
+        # + 12 B per query window; hits counted exactly on the first queries
+        # and scaled by windows)
         fwd, rc, counts = engine.pack(spec, x_dev, l_dev)
         n_win = int(counts.sum().item())
         nsample = min(B, 4096)
@@ -452,7 +454,12 @@ def run_b200(args):
         win_s = int(counts[:nsample].sum().item())
         hits = hits_s * n_win / max(win_s, 1)
         lookups = n_win * int(index.masks.numel())
-        alg_bytes = lookups * 8 + hits * 4 + 12 * n_win
+        entry_bytes = 2 if (not spec.base.weighted and index.tile_svs <= 65536) else 4
+        alg_bytes = lookups * 8 + hits * entry_bytes + 12 * n_win
+        # DRAM traffic of the launch: ncu's dram__bytes_read.sum +
+        # dram__bytes_write.sum on a 2,000-query launch of this workload
+        # (1.4475e9 B; the SV index stays in L2), scaled by queries
+        traffic = 1.4475e9 * B / 2000
         score_ms = query_ms
         achieved = alg_bytes / (score_ms / 1e3) / 1e9
         peaks = {}
@@ -468,7 +475,8 @@ def run_b200(args):
             "config": {"workload": WORKLOAD, "queries_per_rank": B, "svs": len(coef), "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (packed queries and the 280 MB SV index exceed 126 MB)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": "ncu dram bytes of a 2,000-query launch, scaled by queries",
                          "kernel": "index_query (fused SV-tile query + RBF + alpha reduce)",
                          "alg_bytes_per_launch": alg_bytes, "hits": hits, "lookups": lookups,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6.65 TB/s"},
