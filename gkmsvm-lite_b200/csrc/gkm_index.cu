@@ -259,7 +259,10 @@ constexpr int Q_THREADS = 1024;
 constexpr int Q_WARPS = Q_THREADS / 32;
 constexpr int LOG_CAP = 64;            // carry events a block can log (16-bit counters)
 constexpr int MASKS_SMEM_MAX = 6144;   // neighbour masks staged in shared memory up to this
-enum { MODE_SCORE = 0, MODE_RAW = 1 };
+// MODE_COUNT: an item covers a range of a row's windows (a row split) and adds
+// its exact per-(SV, level) counts into gcount; a finish kernel turns the
+// summed counts into K_raw, profiles or scores.
+enum { MODE_SCORE = 0, MODE_RAW = 1, MODE_COUNT = 2 };
 enum { EV_LOWCARRY = 0, EV_WRAP = 1 };
 
 struct QueryArgs {
@@ -286,6 +289,9 @@ struct QueryArgs {
     unsigned int *queue;  // work-queue head: items (tile, row) handed out tile-major
     int64_t B;            // rows
     int tiles;
+    int nsplit;           // items per (row, tile): window ranges of split_w windows
+    int split_w;
+    unsigned long long *gcount;  // MODE_COUNT: [B, S, nlev] summed counts
     // score
     const double *inv_dx;
     const double *inv_ds;
@@ -389,9 +395,12 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
     if (threadIdx.x == 0) item_s = atomicAdd(a.queue, 1u);
     __syncthreads();
     const unsigned int item = item_s;
-    if ((int64_t)item >= a.B * a.tiles) break;
-    const int t = (int)(item / a.B);
-    const int64_t r = item - (int64_t)t * a.B;
+    const int64_t per_tile = a.B * a.nsplit;
+    if ((int64_t)item >= per_tile * a.tiles) break;
+    const int t = (int)(item / per_tile);
+    const int64_t rem = item - (int64_t)t * per_tile;
+    const int64_t r = rem / a.nsplit;
+    const int ks = (int)(rem - r * a.nsplit);
     const int64_t row = a.order ? a.order[r] : r;
     const int64_t s0 = (int64_t)t * St;
     const int ns = (int)min((int64_t)St, a.S - s0);
@@ -399,6 +408,9 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
     if (MODE == MODE_RAW && s0 + ns <= lo_g) continue;  // tile wholly below the diagonal
     const uint32_t lo = (uint32_t)(lo_g > s0 ? lo_g - s0 : 0);
     const int n = a.cx[row];
+    // this item's windows [i0, i1) of the row (the whole row unless split)
+    const int i0 = min(n, ks * a.split_w), i1 = min(n, i0 + a.split_w);
+    if (MODE == MODE_COUNT && i0 >= i1) continue;
     const uint32_t *x = a.bx + row * a.W;
     const uint32_t *off = a.off + (int64_t)t * a.n_lmers;
     const double inv_dx = MODE == MODE_SCORE ? a.inv_dx[row] : 0.0;
@@ -412,7 +424,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         if (threadIdx.x == 0) nlog = 0;
         __syncthreads();
         const uint32_t id_lo = max((uint32_t)sub_lo, lo), id_hi = (uint32_t)(sub_lo + sub_n);
-        for (int i = warp; i < n; i += Q_WARPS) {
+        for (int i = i0 + warp; i < i1; i += Q_WARPS) {
             const uint32_t u = x[i];
             const uint32_t wq = WEIGHTED ? (a.wq ? (uint32_t)a.wq[row * a.W + i] : gkm_wt(a.wd, n, i)) : 1u;
             // per lane: its mask's bucket and counter slot (C16: word base and
@@ -478,6 +490,15 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         }
         __syncthreads();
         const int nl = min(nlog, LOG_CAP);
+        if (MODE == MODE_COUNT) {
+            for (int s = sub_lo + threadIdx.x; s < sub_lo + sub_n; s += Q_THREADS) {
+                unsigned long long *g = a.gcount + (row * a.S + s0 + s) * a.nlev;
+                for (int m = 0; m < a.nlev; m++) {
+                    const int64_t c = read_count<C16>(sm_acc, sm_log, nl, m, stride, s - sub_lo);
+                    if (c) atomicAdd(g + m, (unsigned long long)c);
+                }
+            }
+        } else
         for (int s = sub_lo + threadIdx.x; s < sub_lo + sub_n; s += Q_THREADS) {
             double k = 0.0;
             for (int m = 0; m < a.nlev; m++)
@@ -713,6 +734,9 @@ static QueryArgs query_args(const gkm_index_t *ix, const uint32_t *bx, const int
     a.cx = cx;
     a.W = W;
     a.diag_offset = -1;
+    a.nsplit = 1;
+    a.split_w = (int)(W > 0x7FFFFFFF ? 0x7FFFFFFF : W);
+    a.gcount = nullptr;
     a.off = ix->offsets;
     a.ent = ix->ent16 ? (const void *)ix->ent16 : (const void *)ix->ent;
     a.masks = ix->masks;
@@ -748,7 +772,7 @@ static void launch_query(unsigned grid, size_t smem, cudaStream_t st, const Quer
 template <int MODE>
 static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cudaStream_t st)
 {
-    if (B * ix->tiles > 0xFFFFFFFFLL - 2LL * gkm_sm_count())
+    if (B * ix->tiles * a.nsplit > 0xFFFFFFFFLL - 2LL * gkm_sm_count())
         return gkm_fail(GKM_ERR_UNSUPPORTED, "too many (row, tile) items for one launch");
     size_t smem = query_fixed_smem(ix->n_masks) + 16 + (size_t)ix->acc_bytes;
     // one resident block per SM, fed by the work queue (a counter of the
@@ -760,7 +784,7 @@ static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cu
     q.queue = ix->queues + slot;
     cudaError_t e0 = cudaMemsetAsync(q.queue, 0, sizeof(unsigned int), st);
     if (e0 != cudaSuccess) return gkm_cuda_status(e0, "index queue");
-    int64_t items = B * ix->tiles;
+    int64_t items = B * ix->tiles * a.nsplit;
     unsigned grid = (unsigned)(items < gkm_sm_count() ? items : gkm_sm_count());
     if (ix->spec.weighted)
         launch_query<true, MODE, false, false>(grid, smem, st, q);
@@ -776,6 +800,95 @@ static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cu
     return GKM_OK;
 }
 
+// Row splits for small batches: when (rows x tiles) items cannot fill the GPU,
+// each row's windows are cut into nsplit ranges of at least 32 windows, so
+// items = rows x tiles x nsplit; the summed counts (B x S x levels x 8 B) are
+// kept within 256 MB.  1: no split.
+static int split_plan(const gkm_index_t *ix, int64_t B, int64_t W)
+{
+    const int64_t items = B * ix->tiles, target = 2LL * gkm_sm_count();
+    if (items >= target || W < 64) return 1;
+    if (B * ix->S * ix->nlev * 8 > (256LL << 20)) return 1;
+    int64_t ns = (target + items - 1) / items;
+    if (ns > W / 32) ns = W / 32;
+    return ns < 2 ? 1 : (int)ns;
+}
+
+// K_raw / profiles / per-(row, tile) score partials from summed counts, each
+// SV's levels in a fixed order (deterministic)
+struct CountFinish {
+    const unsigned long long *g;
+    int64_t B, S;
+    int nlev, l, tiles, tile_svs;
+    double h[16];
+    double *raw;
+    uint64_t *profile;
+    const double *inv_dx, *inv_ds, *coef;
+    double gamma;
+    int rbf;
+    double *partial;
+};
+
+__global__ void count_finish_raw(CountFinish f)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= f.B * f.S) return;
+    const unsigned long long *g = f.g + i * f.nlev;
+    double k = 0.0;
+    for (int m = 0; m < f.nlev; m++) k += f.h[m] * (double)g[m];
+    if (f.raw) f.raw[i] = k;
+    if (f.profile)
+        for (int m = 0; m <= f.l; m++) f.profile[i * (f.l + 1) + m] = m < f.nlev ? (uint64_t)g[m] : 0;
+}
+
+__global__ void count_finish_score(CountFinish f)
+{
+    __shared__ double red[32];
+    const int t = blockIdx.x;
+    const int64_t row = blockIdx.y;
+    const int64_t s0 = (int64_t)t * f.tile_svs, s1 = min(f.S, s0 + f.tile_svs);
+    const double inv_dx = f.inv_dx[row];
+    double part = 0.0;
+    for (int64_t s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        const unsigned long long *g = f.g + (row * f.S + s) * f.nlev;
+        double k = 0.0;
+        for (int m = 0; m < f.nlev; m++) k += f.h[m] * (double)g[m];
+        const double kn = k * inv_dx * f.inv_ds[s];
+        part += f.coef[s] * (f.rbf ? exp(f.gamma * (kn - 1.0)) : kn);
+    }
+    part = gkm_block_sum(part, red);
+    if (threadIdx.x == 0) f.partial[row * f.tiles + t] = part;
+}
+
+// the split query into freshly zeroed counts (caller frees *g)
+static int query_split(const gkm_index_t *ix, QueryArgs a, int64_t B, int64_t W, int nsplit,
+                       unsigned long long **g, cudaStream_t st)
+{
+    const size_t bytes = sizeof(unsigned long long) * (size_t)(B * ix->S * ix->nlev);
+    if (cudaMallocAsync((void **)g, bytes, st) != cudaSuccess) return gkm_fail(GKM_ERR_OOM, "split counts");
+    cudaError_t e = cudaMemsetAsync(*g, 0, bytes, st);
+    if (e != cudaSuccess) return gkm_cuda_status(e, "split counts");
+    a.nsplit = nsplit;
+    a.split_w = (int)((W + nsplit - 1) / nsplit);
+    a.gcount = *g;
+    a.order = nullptr;
+    return query_launch<MODE_COUNT>(ix, a, B, st);
+}
+
+static CountFinish count_finish_args(const gkm_index_t *ix, const unsigned long long *g, int64_t B)
+{
+    CountFinish f = {};
+    f.g = g;
+    f.B = B;
+    f.S = ix->S;
+    f.nlev = ix->nlev;
+    f.l = ix->spec.l;
+    f.tiles = ix->tiles;
+    f.tile_svs = ix->tile_svs;
+    for (int m = 0; m < 16; m++) f.h[m] = ix->spec.h[m];
+    return f;
+}
+
 extern "C" int gkm_index_pairwise(const gkm_index_t *ix, const uint32_t *bx, const int32_t *cx, int64_t B,
                                   int64_t W, int64_t diag_offset, double *raw, uint64_t *profile,
                                   gkm_stream_t stream)
@@ -786,7 +899,21 @@ extern "C" int gkm_index_pairwise(const gkm_index_t *ix, const uint32_t *bx, con
     a.diag_offset = diag_offset;
     a.raw = raw;
     a.profile = profile;
-    return query_launch<MODE_RAW>(ix, a, B, (cudaStream_t)stream);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nsplit = diag_offset < 0 ? split_plan(ix, B, W) : 1;
+    if (nsplit == 1) return query_launch<MODE_RAW>(ix, a, B, st);
+    unsigned long long *g = nullptr;
+    int s = query_split(ix, a, B, W, nsplit, &g, st);
+    if (s == GKM_OK) {
+        CountFinish f = count_finish_args(ix, g, B);
+        f.raw = raw;
+        f.profile = profile;
+        count_finish_raw<<<(unsigned)((B * ix->S + 255) / 256), 256, 0, st>>>(f);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) s = gkm_cuda_status(e, "count_finish_raw");
+    }
+    if (g) cudaFreeAsync(g, st);
+    return s;
 }
 
 extern "C" int gkm_index_score(const gkm_index_t *ix, const uint32_t *bx, const int32_t *cx, int64_t B,
@@ -809,7 +936,27 @@ extern "C" int gkm_index_score(const gkm_index_t *ix, const uint32_t *bx, const 
     a.gamma = gamma;
     a.rbf = rbf;
     a.partial = partial;
-    int s = query_launch<MODE_SCORE>(ix, a, B, st);
+    const int nsplit = split_plan(ix, B, W);
+    int s = GKM_OK;
+    if (nsplit == 1) {
+        s = query_launch<MODE_SCORE>(ix, a, B, st);
+    } else {
+        unsigned long long *g = nullptr;
+        s = query_split(ix, a, B, W, nsplit, &g, st);
+        if (s == GKM_OK) {
+            CountFinish f = count_finish_args(ix, g, B);
+            f.inv_dx = inv_dx;
+            f.inv_ds = inv_ds;
+            f.coef = coef;
+            f.gamma = gamma;
+            f.rbf = rbf;
+            f.partial = partial;
+            count_finish_score<<<dim3((unsigned)ix->tiles, (unsigned)B), 256, 0, st>>>(f);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) s = gkm_cuda_status(e, "count_finish_score");
+        }
+        if (g) cudaFreeAsync(g, st);
+    }
     if (s == GKM_OK) {
         finish_scores<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(partial, B, ix->tiles, bias, scores);
         cudaError_t e = cudaGetLastError();

@@ -344,7 +344,10 @@ def test_counter_carries_are_exact():
     raw, prof = ix1.pairwise(fwd, counts, profile=True)
     np.testing.assert_array_equal(_np(prof)[..., :4].astype(np.uint64), want_prof[..., :4])
     ix1.close()
-    # ten poly-A SVs in one tile: the log overflows and the query reruns
+    # ten poly-A SVs in one tile, each row whole in one block (300 rows: enough
+    # items that no row is split): the log overflows and the query reruns
+    xr = np.repeat(x, 100, axis=0)
+    fwd, rc, counts = engine.pack(spec, torch.from_numpy(xr).cuda(), None)
     inv_dx = 1.0 / torch.sqrt(engine.self_kernel(spec, fwd, rc, counts))
     before = index.counters()
     index.score(fwd, counts, inv_dx, m._inv_ds(), m._sv_coef(), 2.0, 1, 0.0, check=False)
