@@ -424,7 +424,12 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         if (threadIdx.x == 0) nlog = 0;
         __syncthreads();
         const uint32_t id_lo = max((uint32_t)sub_lo, lo), id_hi = (uint32_t)(sub_lo + sub_n);
-        for (int i = i0 + warp; i < i1; i += Q_WARPS) {
+        // work units (window, mask group): rows of fewer windows than warps
+        // share each window's masks among g warps, so every warp has work
+        const int nwin = i1 - i0;
+        const int g = nwin >= Q_WARPS ? 1 : max(1, min(Q_WARPS / max(nwin, 1), (n_masks + 31) / 32));
+        for (int wu = warp; wu < nwin * g; wu += Q_WARPS) {
+            const int i = i0 + wu / g, kg = wu - (wu / g) * g;
             const uint32_t u = x[i];
             const uint32_t wq = WEIGHTED ? (a.wq ? (uint32_t)a.wq[row * a.W + i] : gkm_wt(a.wd, n, i)) : 1u;
             // per lane: its mask's bucket and counter slot (C16: word base and
@@ -444,10 +449,10 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                 b0 = __ldg(off + v);
                 e0 = __ldg(off + v + 1);
             };
-            if (lane < n_masks) lane_mask(lane, beg, end, base, add, fmask);
-            for (int c0 = 0; c0 < n_masks; c0 += 32) {
+            if (kg * 32 + lane < n_masks) lane_mask(kg * 32 + lane, beg, end, base, add, fmask);
+            for (int c0 = kg * 32; c0 < n_masks; c0 += 32 * g) {
                 uint32_t nbeg = 0, nend = 0, nbase = 0, nadd = 0, nfm = 0;
-                const int cn = c0 + 32 + lane;
+                const int cn = c0 + 32 * g + lane;
                 if (cn < n_masks) lane_mask(cn, nbeg, nend, nbase, nadd, nfm);
                 // the bucket in aligned blocks of four entries, one vector load each
                 for (uint32_t e = beg & ~3u; __any_sync(GKM_FULL, e < end); e += 4) {
@@ -1018,10 +1023,22 @@ extern "C" int gkm_index_count(const gkm_index_t *ix, const uint32_t *bx, const 
 
 // ---------------------------------------------------------------------------
 // ISM through the index (kernels/lmer_index_cpu.py:203-285): per (position p,
-// row b), the windows covering p before (set 0) and after each substitution v
-// (sets 1..4) are queried as rows of <= l windows that keep their slot weights
-// (ism.py:276-295); then K(mutant, s) = ref[b, s] + K(set v, s) - K(set 0, s).
+// row b), the windows covering p before (set 0) and after each of the three
+// substitutions (sets 1..3) are queried as rows of <= l windows that keep their
+// slot weights (ism.py:276-295); then K(mutant, s) = ref[b, s] + K(set v, s) -
+// K(set 0, s), and the reference base's own delta is exactly 0.
 // ---------------------------------------------------------------------------
+
+// the base at p as packed in the first window covering it (-1: none covers p)
+__device__ __forceinline__ int ism_ref_base(const uint32_t *fwd, int64_t b, int64_t W, int64_t p, int a_s, int a_e)
+{
+    return a_e > a_s ? (int)((fwd[b * W + a_s] >> (2 * (p - a_s))) & 3u) : -1;
+}
+
+// sets per (position, row): 0 = the reference windows covering p; 1..3 = the
+// same windows with the three other bases at p, in increasing base order (the
+// reference base's own set would repeat set 0, and its delta is exactly 0)
+constexpr int ISM_SETS = 4;
 
 __global__ void ism_sets_kernel(gkm_spec spec, const uint32_t *__restrict__ fwd, const int32_t *__restrict__ cnt,
                                 int64_t B, int64_t W, int64_t p0, int64_t nitems, uint32_t *__restrict__ rows,
@@ -1035,8 +1052,10 @@ __global__ void ism_sets_kernel(gkm_spec spec, const uint32_t *__restrict__ fwd,
     int a_s = (int)(p - l + 1 > 0 ? p - l + 1 : 0);
     int a_e = (int)(p + 1 < n ? p + 1 : n);
     int na = a_e > a_s ? a_e - a_s : 0;
-    for (int r = 0; r < 5; r++) {
-        int64_t row = it * 5 + r;
+    const int xp = ism_ref_base(fwd, b, W, p, a_s, a_e);
+    for (int r = 0; r < ISM_SETS; r++) {
+        int64_t row = it * ISM_SETS + r;
+        const int v = r == 0 ? -1 : (r - 1) + ((r - 1) >= xp ? 1 : 0);
         rcount[row] = na;
         for (int j = 0; j < l; j++) {
             uint32_t w = GKM_PAD;
@@ -1046,7 +1065,7 @@ __global__ void ism_sets_kernel(gkm_spec spec, const uint32_t *__restrict__ fwd,
                 w = fwd[b * W + i];
                 if (r > 0) {
                     uint32_t sh = 2u * (uint32_t)(p - i);
-                    w = (w & ~(3u << sh)) | ((uint32_t)(r - 1) << sh);
+                    w = (w & ~(3u << sh)) | ((uint32_t)v << sh);
                 }
                 wt = spec.weighted ? (uint8_t)gkm_wt(spec.wd, n, i) : 1;
             }
@@ -1069,18 +1088,16 @@ __global__ void ism_index_finish(const double *__restrict__ kset, int64_t S, con
     int n = cnt[b];
     int a_s = (int)(p - l + 1 > 0 ? p - l + 1 : 0);
     int a_e = (int)(p + 1 < n ? p + 1 : n);
-    // the base at p as packed in the first window covering it
-    int xp = a_e > a_s ? (int)((fwd[b * W + a_s] >> (2 * (p - a_s))) & 3u) : -1;
-    const double *k0 = kset + (it * 5) * S;
+    const int xp = ism_ref_base(fwd, b, W, p, a_s, a_e);
+    const double *k0 = kset + (it * ISM_SETS) * S;
     const double *rr = ref + b * S;
     for (int v = 0; v < 4; v++) {
         double z = inv_dmut[((int64_t)v * L + p) * B + b];
-        bool same = a_e <= a_s || (v == xp && z == inv_dx[b]);
-        if (same) {  // the reference's windows and norm: exactly 0
+        if (a_e <= a_s || v == xp) {  // the reference itself: exactly 0
             if (threadIdx.x == 0) out[(b * 4 + v) * L + p] = 0.0;
             continue;
         }
-        const double *kv = kset + (it * 5 + 1 + v) * S;
+        const double *kv = kset + (it * ISM_SETS + 1 + v - (v > xp ? 1 : 0)) * S;
         double acc = 0.0;
         for (int64_t s = threadIdx.x; s < S; s += blockDim.x) {
             double k = (rr[s] + (kv[s] - k0[s])) * z * inv_ds[s];
@@ -1102,7 +1119,7 @@ extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, con
     cudaStream_t st = (cudaStream_t)stream;
     const int l = ix->spec.l;
     const int64_t S = ix->S;
-    int64_t per_item = 5 * S * (int64_t)sizeof(double);
+    int64_t per_item = ISM_SETS * S * (int64_t)sizeof(double);
     int64_t chunk = (1LL << 30) / per_item;
     if (chunk < 1) chunk = 1;
     int64_t total = L * B;
@@ -1115,10 +1132,10 @@ extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, con
     uint8_t *rw = nullptr;
     double *kset = nullptr;
     int s = GKM_OK;
-    if (cudaMallocAsync(&rows, sizeof(uint32_t) * chunk * 5 * l, st) != cudaSuccess ||
-        cudaMallocAsync(&rc, sizeof(int32_t) * chunk * 5, st) != cudaSuccess ||
-        cudaMallocAsync(&rw, chunk * 5 * l, st) != cudaSuccess ||
-        cudaMallocAsync(&kset, sizeof(double) * chunk * 5 * S, st) != cudaSuccess)
+    if (cudaMallocAsync(&rows, sizeof(uint32_t) * chunk * ISM_SETS * l, st) != cudaSuccess ||
+        cudaMallocAsync(&rc, sizeof(int32_t) * chunk * ISM_SETS, st) != cudaSuccess ||
+        cudaMallocAsync(&rw, chunk * ISM_SETS * l, st) != cudaSuccess ||
+        cudaMallocAsync(&kset, sizeof(double) * chunk * ISM_SETS * S, st) != cudaSuccess)
         s = gkm_fail(GKM_ERR_OOM, "ISM scratch");
     for (int64_t p0 = 0; s == GKM_OK && p0 < L; p0 += chunk / B) {
         int64_t np = chunk / B;
@@ -1134,7 +1151,7 @@ extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, con
         QueryArgs a = query_args(ix, rows, rc, l);
         a.wq = ix->spec.weighted ? rw : nullptr;
         a.raw = kset;
-        if ((s = query_launch<MODE_RAW>(ix, a, nitems * 5, st)) != GKM_OK) break;
+        if ((s = query_launch<MODE_RAW>(ix, a, nitems * ISM_SETS, st)) != GKM_OK) break;
         ism_index_finish<<<(unsigned)nitems, 256, 0, st>>>(kset, S, fwd, counts, B, W, L, l, p0, ref_raw, ref_score,
                                                            inv_dx, inv_dmut, inv_ds, coef, gamma, rbf, out);
         e = cudaGetLastError();
