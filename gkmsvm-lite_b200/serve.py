@@ -9,8 +9,11 @@ refused), merges every predict and variant row of the batch into one
 graph-captured scoring pass, and keeps up to two such passes in flight on
 separate streams, so requests that arrive while a batch runs are admitted as
 soon as a slot frees up.  ISM and GkmExplain requests run on their own worker
-stream beside the scoring passes.  Every request's latency (submit to result)
-is recorded; stats() gives p50/p99 per request type and sequences per second.
+stream beside the scoring passes; the requests of one kind (and explain mode)
+already waiting when the worker is free run as one batched call (up to
+max_side_rows rows), so a burst of them shares the device.  Every request's
+latency (submit to result) is recorded; stats() gives p50/p99 per request type
+and sequences per second.
 
 The scheduling is independent of the device work: a backend object runs the
 batches (GpuBackend here; the tests drive the same loop with a host fake).
@@ -60,12 +63,15 @@ class GkmServer:
     """Continuous-batching request loop over one model (see the module doc)."""
 
     def __init__(self, backend, *, max_batch_rows: int = 8192, max_inflight: int = 2,
-                 memory_reserve: int = 2 << 30, max_wait_s: float = 0.002):
+                 memory_reserve: int = 2 << 30, max_wait_s: float = 0.002, max_side_rows: int = 64):
         self.backend = backend
         self.max_batch_rows = max_batch_rows
         self.max_inflight = max_inflight
         self.memory_reserve = memory_reserve
         self.max_wait_s = max_wait_s
+        self.max_side_rows = max_side_rows
+        self.side_memory_wait_s = 30.0
+        self.side_batches: list[int] = []  # requests per side call
         self._in: queue.Queue = queue.Queue()
         self._side: queue.Queue = queue.Queue()
         self._waiting: list[Request] = []
@@ -190,26 +196,60 @@ class GkmServer:
                 r.future.set_result(res)
 
     def _side_loop(self):
-        while not (self._stop.is_set() and self._side.empty()):
+        pending: list[Request] = []
+        batched = hasattr(self.backend, "run_side_batch")
+        call_bytes = getattr(self.backend, "side_call_bytes", 0)
+        while not (self._stop.is_set() and self._side.empty() and not pending):
             try:
-                r = self._side.get(timeout=0.01)
+                pending.append(self._side.get(timeout=0.01 if not pending else 0.0005))
+                while True:
+                    pending.append(self._side.get_nowait())
             except queue.Empty:
+                pass
+            if not pending:
                 continue
-            while r.bytes > self._free_memory():
-                if self._stop.is_set():
+            # the oldest request's kind (and explain mode), with every waiting
+            # request of the same kind that fits the row budget
+            head = pending[0]
+            free = self._free_memory()
+            batch, rows, need = [], 0, call_bytes
+            for r in list(pending):
+                if r.kind != head.kind or r.mode != head.mode:
+                    continue
+                if batch and (not batched or rows + r.rows > self.max_side_rows or need + r.bytes > free):
                     break
+                batch.append(r)
+                rows += r.rows
+                need += r.bytes
+            for r in batch:
+                pending.remove(r)
+            # the oldest request alone may still need more than is free: wait
+            # for memory (bounded), then refuse it
+            deadline = time.perf_counter() + self.side_memory_wait_s
+            while need > self._free_memory() and time.perf_counter() < deadline and not self._stop.is_set():
                 time.sleep(0.001)
-            r.t_start = time.perf_counter()
+            if need > self._free_memory():
+                self.rejected += len(batch)
+                for r in batch:
+                    r.future.set_exception(AdmissionError("not enough free device memory for this request"))
+                continue
+            t = time.perf_counter()
+            for r in batch:
+                r.t_start = t
             try:
-                res = self.backend.run_side(r)
+                results = self.backend.run_side_batch(batch) if batched else [self.backend.run_side(batch[0])]
             except Exception as e:
-                r.future.set_exception(e)
+                for r in batch:
+                    r.future.set_exception(e)
                 continue
             now = time.perf_counter()
             with self._lock:
-                self._lat[r.kind].append(now - r.t_submit)
-                self._seqs += r.rows
-            r.future.set_result(res)
+                self.side_batches.append(len(batch))
+                for r in batch:
+                    self._lat[r.kind].append(now - r.t_submit)
+                    self._seqs += r.rows
+            for r, res in zip(batch, results):
+                r.future.set_result(res)
 
     def stats(self) -> dict:
         with self._lock:
@@ -219,10 +259,14 @@ class GkmServer:
             out["all"] = _percentiles(allv)
             out["seqs_per_sec"] = self._seqs / wall if wall > 0 else 0.0
             out["admitted"], out["deferred"], out["rejected"] = self.admitted, self.deferred, self.rejected
+            out["side_calls"] = len(self.side_batches)
+            out["side_requests_per_call"] = (float(np.mean(self.side_batches)) if self.side_batches else 0.0)
             return out
 
 
 class GpuBackend:
+    side_call_bytes = 3 << 29  # an ISM / explain call's chunked scratch (1.5 GiB)
+
     """Runs a GkmServer's batches on the model's GPU: scoring rows through
     BatchedScorer (two instances, one per in-flight slot, each on its own
     stream), ISM and GkmExplain through the model's own calls on a side stream."""
@@ -260,7 +304,14 @@ class GpuBackend:
             n, L = x.shape
             r.rows = n
         # packed windows + scratch of its rows (ISM: mutant window sets too)
-        r.bytes = r.rows * L * 16 + (L * 4 * 5 * 8 * self.model.num_support_vectors if r.kind == "ism" else 0)
+        # device memory while it runs: packed windows and float64 outputs; an
+        # explain row also holds its [4, l] window parts and (RBF) its SV
+        # weights.  A side call's own scratch (ISM mutant kernel rows, chunked
+        # to about 1 GiB) is side_call_bytes, counted once per call.
+        S = self.model.num_support_vectors
+        per_row = {"predict": L * 16, "score_variants": L * 16, "ism": L * 48,
+                   "explain": L * (48 + 8 * 4 * self.model.kernel.l) + 8 * S}[r.kind]
+        r.bytes = r.rows * per_row
 
     def launch_scoring(self, batch):
         torch = self.torch
@@ -318,13 +369,32 @@ class GpuBackend:
         return out
 
     def run_side(self, r: Request):
+        return self.run_side_batch([r])[0]
+
+    def run_side_batch(self, reqs):
+        """One ISM or GkmExplain call over every row of reqs (same kind and
+        mode), rows padded to the widest; each request gets its own rows at its
+        own width (a row's results do not depend on the rows beside it)."""
         from .explain import gkmexplain
         from .ism import ism
 
         torch = self.torch
+        L = max(int(np.asarray(r.x).shape[1]) for r in reqs)
+        xs, lens, spans, a = [], [], [], 0
+        for r in reqs:
+            x = np.asarray(r.x)
+            n, w = x.shape
+            pad = np.zeros((n, L), np.uint8)
+            pad[:, :w] = x
+            xs.append(pad)
+            lens.append(np.full(n, w, np.int64) if r.lengths is None else np.asarray(r.lengths, np.int64))
+            spans.append((a, n, w))
+            a += n
+        X, lengths = np.concatenate(xs), np.concatenate(lens)
         with torch.cuda.stream(self.side_stream):
-            if r.kind == "ism":
-                res = ism(self.model, r.x, lengths=r.lengths)
+            if reqs[0].kind == "ism":
+                res = ism(self.model, X, lengths=lengths)
             else:
-                res = gkmexplain(self.model, r.x, lengths=r.lengths, mode=r.mode)
-            return res.cpu().numpy()
+                res = gkmexplain(self.model, X, lengths=lengths, mode=reqs[0].mode)
+            host = res.cpu().numpy()
+        return [host[a:a + n, :, :w] for a, n, w in spans]

@@ -96,3 +96,49 @@ def test_bad_requests_fail_alone():
         with pytest.raises(AdmissionError):
             too_big.result(5)
         np.testing.assert_array_equal(ok.result(5), [[3.0], [3.0]])
+
+
+class FakeBatchBackend(FakeBackend):
+    """Side requests through run_side_batch: one call per batch, recorded."""
+
+    def __init__(self, **kw):
+        super().__init__(**kw)
+        self.side_calls = []
+
+    def run_side_batch(self, reqs):
+        with self.lock:
+            self.side_calls.append([(r.kind, r.rows) for r in reqs])
+        time.sleep(self.delay)
+        return [np.asarray(r.x) * 2.0 for r in reqs]
+
+
+def test_waiting_side_requests_share_one_call():
+    be = FakeBatchBackend(delay=0.05)
+    srv = GkmServer(be, max_side_rows=8).start()
+    rng = np.random.default_rng(3)
+    xs = [rng.integers(0, 4, (1 + i % 2, 20 + i)) for i in range(12)]
+    futs = [srv.submit("ism", x) for x in xs] + [srv.submit("explain", xs[0], mode="perturbation")]
+    for x, f in zip(xs, futs):
+        np.testing.assert_array_equal(f.result(10), x * 2.0)
+    np.testing.assert_array_equal(futs[-1].result(10), xs[0] * 2.0)
+    srv.stop()
+    # the first call takes what waited then; later ones gather the burst
+    assert max(len(c) for c in be.side_calls) > 1
+    assert all(len({k for k, _ in c}) == 1 for c in be.side_calls)  # one kind per call
+    assert all(sum(n for _, n in c) <= 8 or len(c) == 1 for c in be.side_calls)  # the row budget
+    st = srv.stats()
+    assert st["ism"]["n"] == 12 and st["explain"]["n"] == 1
+
+
+def test_side_request_beyond_free_memory_is_refused():
+    be = FakeBatchBackend(free=10_000, delay=0.01)
+    srv = GkmServer(be, memory_reserve=0)
+    srv.side_memory_wait_s = 0.2
+    srv.start()
+    huge = srv.submit("ism", np.zeros((20, 3)))  # 20,000 B > all free memory
+    ok = srv.submit("ism", np.ones((2, 3)))
+    with pytest.raises(AdmissionError):
+        huge.result(10)
+    np.testing.assert_array_equal(ok.result(10), np.full((2, 3), 2.0))
+    srv.stop()
+    assert srv.stats()["rejected"] == 1
