@@ -69,6 +69,8 @@ SIGNATURES = {
     "gkm_raw_score": [P, I64, I64, P, P, P, D, I32, D, P, P],
     "gkm_impact": [P, I64, I64, P, P, P, D, I32, P, P],
     "gkm_explain_lmer": [SPEC, P, P, I64, I64, I64, P, P, P, P, P, I32, P, P, I32, P, P],
+    "gkm_explain_table_build": [SPEC, P, P, P, P, P],
+    "gkm_explain_table": [SPEC, P, P, P, I64, I64, I64, P, I32, P, P],
     "gkm_gram_finish": [P, I64, I64, P, P, D, I32, I32, P, P],
 }
 

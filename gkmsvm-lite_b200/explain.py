@@ -7,6 +7,12 @@ times the neighbour's weight to each of its positions.  The weight of a
 neighbour v is V[v] = sum_s coef_s / sqrt(K(sv, sv)) (occurrences of v in sv_s
 and its RC) for linear kernels, and for RBF kernels the per-query SV weights
 summed over the l-mer index's entries of v (gkm_explain_lmer).
+
+Linear kernels can instead read every window's attribution from the explain
+table (explain/table.py): [4^l, 4, l] float64 built once per mode on the GPU by
+Walsh-Hadamard transforms (gkm_explain_table_build) and cached on the model;
+use_explain_table = True / False / "auto" (built once a call explains enough
+rows to pay for it, and at most 2 GiB).
 """
 
 from __future__ import annotations
@@ -62,6 +68,39 @@ def _explain_V(model) -> torch.Tensor:
     return c["explain_V"]
 
 
+# explain table limits and cost model ("auto"): build cost per entry of 4^l x l
+# and the direct l-mer path's cost per query window, measured on B200 at l=11
+# (a first call that builds V and the table: 0.17 s; the direct path: ~3e6
+# windows/s, the table ~3e7), so a call of ~300k windows pays for it
+_EXPLAIN_TABLE_MAX_L = 12
+_EXPLAIN_TABLE_BYTES = 2 * 2**30
+_TABLE_BUILD_S_PER_ENTRY = 1e-9
+_DIRECT_S_PER_WINDOW = 1.5e-7
+
+
+def _explain_table(model, n_windows: int, perturbation: bool, dev):
+    """The cached explain table of this mode, built if use_explain_table calls
+    for it, or None (RBF models have none)."""
+    use = model.use_explain_table
+    kernel = model.kernel
+    base = kernel.base
+    l = base.l
+    if use is False or isinstance(kernel, RbfKernel) or l > _EXPLAIN_TABLE_MAX_L:
+        return None
+    tables = model._explain_tables
+    if perturbation not in tables:
+        n = 4 ** l
+        if use == "auto" and (n * 4 * l * 8 > _EXPLAIN_TABLE_BYTES
+                              or n_windows * _DIRECT_S_PER_WINDOW < _TABLE_BUILD_S_PER_ENTRY * n * l):
+            return None
+        _, ta, tb = _explain_masks(model, perturbation, dev)
+        A = torch.empty((n, 4, l), dtype=torch.float64, device=dev)
+        call("gkm_explain_table_build", model._spec().ref, ptr(_explain_V(model)), ptr(ta), ptr(tb), ptr(A),
+             stream_handle())
+        tables[perturbation] = A
+    return tables[perturbation]
+
+
 def gkmexplain(model, x, *, mode="importance", lengths=None, batch_size=50, verbose=False) -> torch.Tensor:
     """[B, 4, L] float64 attributions (explain/core.py:34-113): importance =
     hypothetical x one-hot (N credited to A), hypothetical, or perturbation."""
@@ -73,18 +112,22 @@ def gkmexplain(model, x, *, mode="importance", lengths=None, batch_size=50, verb
     short = short_rows(lengths, model.kernel.base.l, "attributions")
     B, L = x.shape
     bs = max(1, int(batch_size)) if batch_size else B
+    # the table (if any) is chosen for the whole call, as the reference does
+    n_windows = int(np.clip(np.asarray(lengths if lengths is not None else np.full(B, L)) - model.kernel.base.l + 1,
+                            0, None).sum())
+    table = _explain_table(model, n_windows, resolved == "perturbation", dev)
     parts = []
     it = range(0, B, bs)
     if verbose:
         from tqdm import tqdm
         it = tqdm(it, desc="GkmExplain")
     for s in it:
-        parts.append(_explain_rows(model, x[s:s + bs], rows(lengths, s, bs), resolved, dev))
+        parts.append(_explain_rows(model, x[s:s + bs], rows(lengths, s, bs), resolved, dev, table))
     out = parts[0] if len(parts) == 1 else torch.cat(parts)
     return per_position(out, lengths, short)
 
 
-def _explain_rows(model, x, lengths, mode, dev):
+def _explain_rows(model, x, lengths, mode, dev, table=None):
     kernel = model.kernel
     base = kernel.base
     spec = model._spec()
@@ -103,7 +146,11 @@ def _explain_rows(model, x, lengths, mode, dev):
     else:
         inv_dx = torch.ones(B, dtype=torch.float64, device=dev)
     V = index = w = None
-    if isinstance(kernel, RbfKernel):
+    if table is not None:
+        out = torch.empty((B, 4, L), dtype=torch.float64, device=dev)
+        call("gkm_explain_table", spec.ref, ptr(table), ptr(fwd), ptr(counts), B, W, L, ptr(inv_dx),
+             int(perturbation), ptr(out), stream_handle())
+    elif isinstance(kernel, RbfKernel):
         index = model._sv_index()
         if index is None:
             raise NotImplementedError("RBF GkmExplain needs the l-mer index")
@@ -114,10 +161,11 @@ def _explain_rows(model, x, lengths, mode, dev):
         w = w.contiguous()
     else:
         V = _explain_V(model)
-    out = torch.empty((B, 4, L), dtype=torch.float64, device=dev)
-    call("gkm_explain_lmer", spec.ref, ptr(fwd), ptr(counts), B, W, L, ptr(inv_dx), ptr(V),
-         None if index is None else index.handle, ptr(w), ptr(masks), int(masks.numel()), ptr(ta), ptr(tb),
-         int(perturbation), ptr(out), stream_handle())
+    if table is None:
+        out = torch.empty((B, 4, L), dtype=torch.float64, device=dev)
+        call("gkm_explain_lmer", spec.ref, ptr(fwd), ptr(counts), B, W, L, ptr(inv_dx), ptr(V),
+             None if index is None else index.handle, ptr(w), ptr(masks), int(masks.numel()), ptr(ta), ptr(tb),
+             int(perturbation), ptr(out), stream_handle())
     if mode == "importance":
         oh = torch.nn.functional.one_hot(xt.long(), 4).permute(0, 2, 1).to(out.dtype)
         out = out * oh

@@ -81,9 +81,11 @@ int gkm_join_pairwise(const gkm_spec *spec, const uint32_t *bx, const int32_t *c
                       uint64_t *profile, gkm_stream_t stream);
 
 /* The same pairwise K_raw and profiles as gkm_join_pairwise, computed on the
- * tensor cores: match counts of 128 query windows x 256 column windows as one
+ * tensor cores: match counts of 128 query windows x 128 column windows as one
  * int8 one-hot product (tcgen05.mma kind::i8, int32 accumulators in tensor
- * memory), pairs within dmax counted exactly in the epilogue.  Needs
+ * memory), pairs within dmax counted exactly in the epilogue.  Allocates up to
+ * 1 GiB of transient device memory per launch round for its pre-built column
+ * tiles.  Needs
  * 0 <= dmax < l <= 15.  error (device int32, caller-zeroed): set non-zero if
  * an MMA did not complete within its wait limit (outputs then undefined).
  * Replaces the same pair loop as gkm_join_pairwise (kernels/packed.py:191-228,
@@ -226,6 +228,23 @@ int gkm_explain_lmer(const gkm_spec *spec, const uint32_t *fwd, const int32_t *c
                      const uint32_t *masks, int32_t n_masks, const double *table_a,
                      const double *table_b, int32_t perturbation, double *out,
                      gkm_stream_t stream);
+
+/* The GkmExplain table of a linear model: A [4^l, 4, l] float64 (caller
+ * allocates, 1.5 GB at l = 11), every l-mer's attribution, from V [4^l] and
+ * the level tables table_a / table_b [l + 2] (device), by radix-4
+ * Walsh-Hadamard transforms.  l <= 12.
+ * Replaces _build_explain_table (explain/table.py:58-113). */
+int gkm_explain_table_build(const gkm_spec *spec, const double *V, const double *table_a,
+                            const double *table_b, double *A, gkm_stream_t stream);
+
+/* GkmExplain attributions out [B, 4, L] read from the table A: one row per
+ * query window (times its window weight), added over the windows covering each
+ * position, times inv_dx.  perturbation: the perturbation-mode table.
+ * Replaces _explain_table_cpu (explain/table.py:117-147). */
+int gkm_explain_table(const gkm_spec *spec, const double *A, const uint32_t *fwd,
+                      const int32_t *counts, int64_t B, int64_t W, int64_t L,
+                      const double *inv_dx, int32_t perturbation, double *out,
+                      gkm_stream_t stream);
 
 /* Normalised, finished Gram [N, M] from raw (upper triangle when symmetric,
  * mirrored exactly).  Replaces compute_gram's tile finish (gram.py:82-106). */
