@@ -300,6 +300,7 @@ def ism_explain_leg(sv, svl, coef, n=512):
         torch.cuda.synchronize()
         out[name] = {"value": n / (a.elapsed_time(b) / 1e3), "unit": "seqs/sec"}
     out["ism_path"] = "l-mer table + fused mutant self-kernels" if model._lmer_table is not None else "index"
+    out["explain_path"] = "explain table (GPU Walsh-Hadamard build, cached)" if model._explain_tables else "l-mer neighbours"
     return out
 
 
