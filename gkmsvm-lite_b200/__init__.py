@@ -1,6 +1,6 @@
 """B200-native (sm_100a) implementation of gkmsvm-lite's pairwise gapped-k-mer
-kernel path: GkmSVM scoring, score_variants, ISM, GkmExplain and the training
-Gram matrix, with the reference's signatures, computed by hand-written CUDA
+kernel path: GkmSVM scoring, score_variants, ISM, GkmExplain, the training
+Gram matrix and the SMO solver's kernel columns, with the reference's signatures, computed by hand-written CUDA
 kernels behind the C ABI of include/gkm_b200.h."""
 
 from .explain import gkmexplain, mutation_impact
@@ -12,10 +12,12 @@ from .kernels import (KERNEL_ALIASES, KERNEL_BUILDERS, CenterWeightedGkmKernel, 
                       DirectGkmKernel, EstTruncGkmKernel, GkmKernel, RbfGkmKernel, RbfKernel,
                       resolve_kernel_type)
 from .model import GkmSVM
+from .solver import KernelColumnCache, smo_solve, smo_svr_solve
 
 __all__ = [
     "GkmSVM", "ism", "gkmexplain", "mutation_impact", "compute_gram", "load_lsgkm_model", "load_model",
     "KERNEL_ALIASES", "KERNEL_BUILDERS", "resolve_kernel_type", "GkmKernel", "DirectGkmKernel",
     "EstTruncGkmKernel", "CenterWeightedGkmKernel", "RbfKernel", "RbfGkmKernel",
-    "CenterWeightedRbfGkmKernel", "as_batch", "encode_codes", "to_codes",
+    "CenterWeightedRbfGkmKernel", "as_batch", "encode_codes", "to_codes", "KernelColumnCache", "smo_solve",
+    "smo_svr_solve",
 ]

@@ -45,6 +45,10 @@ D = ctypes.c_double
 SPEC = ctypes.POINTER(GkmSpec)
 
 # name -> argument types (all return int status)
+# gkm_smo_solve's kernel-column provider: (count, indices, out, ctx) -> status
+COLUMNS_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                              ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
+
 SIGNATURES = {
     "gkm_version": [],
     "gkm_device_info": [P, P],
@@ -71,6 +75,7 @@ SIGNATURES = {
     "gkm_explain_lmer": [SPEC, P, P, I64, I64, I64, P, P, P, P, P, I32, P, P, I32, P, P],
     "gkm_explain_table_build": [SPEC, P, P, P, P, P],
     "gkm_explain_table": [SPEC, P, P, P, I64, I64, I64, P, I32, P, P],
+    "gkm_smo_solve": [I32, I32, P, P, P, D, D, D, I64, I32, I32, COLUMNS_CB, P, P, P, P, I32],
     "gkm_gram_finish": [P, I64, I64, P, P, D, I32, I32, P, P],
 }
 

@@ -1,8 +1,9 @@
 """Build recipe of the CUDA library: nvcc for sm_100a, output in-tree.
 
 ``python -m gkmsvm_lite_b200.build`` (or ``build()``) compiles every
-``csrc/*.cu`` into an object and links ``_build/libgkm_b200.so`` next to this
-file.  Objects are rebuilt only when their source or a header is newer.
+``csrc/*.cu`` (nvcc) and ``csrc/*.cpp`` (host C++, g++) into an object and
+links ``_build/libgkm_b200.so`` next to this file.  Objects are rebuilt only
+when their source or a header is newer.
 """
 
 from __future__ import annotations
@@ -24,6 +25,7 @@ NVCC_FLAGS = [
     "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills",
 ]
+CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall"]
 
 
 def _nvcc() -> str:
@@ -44,24 +46,29 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     os.makedirs(OUT, exist_ok=True)
     nvcc = _nvcc()
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu"))) + sorted(glob.glob(os.path.join(CSRC, "*.cpp")))
+    cxx = os.environ.get("CXX", "g++")
     jobs = []
+    objs = []
     for src in srcs:
-        obj = os.path.join(OUT, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(OUT, os.path.splitext(os.path.basename(src))[0] + ".o")
+        objs.append(obj)
         if _stale(obj, src, headers):
-            jobs.append([nvcc, *NVCC_FLAGS, *(extra or []), "-c", src, "-o", obj])
+            if src.endswith(".cu"):
+                jobs.append([nvcc, *NVCC_FLAGS, *(extra or []), "-c", src, "-o", obj])
+            else:
+                jobs.append([cxx, *CXX_FLAGS, "-I", INCLUDE, "-c", src, "-o", obj])
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if verbose or r.returncode:
             sys.stderr.write(r.stdout + r.stderr)
         if r.returncode:
-            raise RuntimeError(f"nvcc failed: {' '.join(cmd[-3:])}")
+            raise RuntimeError(f"{os.path.basename(cmd[0])} failed: {' '.join(cmd[-3:])}")
         return r.stderr
 
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         list(ex.map(run, jobs))
-    objs = [os.path.join(OUT, os.path.basename(s)[:-3] + ".o") for s in srcs]
     if jobs or not os.path.exists(LIB):
         run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB,
              "-lcudart"])

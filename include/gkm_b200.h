@@ -252,6 +252,24 @@ int gkm_gram_finish(const double *raw, int64_t N, int64_t M, const double *dx,
                     const double *dy, double gamma, int32_t rbf, int32_t symmetric,
                     double *out, gkm_stream_t stream);
 
+/* Kernel-column provider of gkm_smo_solve: writes, for k < count, column
+ * idx[k] of the normalized kernel (K(:, idx[k]), N doubles, HOST memory) to
+ * out[k * N ...]; returns 0, or non-zero to stop the solver. */
+typedef int (*gkm_columns_cb)(int32_t count, const int32_t *idx, double *out, void *ctx);
+
+/* SMO training over n dual variables of N sequences (HOST arrays): signs y
+ * [n] (+1/-1), linear term p [n], variable t using column t mod N; C-SVC is
+ * n = N, p = -1; epsilon-SVR is n = 2N, y = (+1, -1), p = (eps - z, eps + z).
+ * diag [N] (nullable: 1) the kernel's diagonal.  Second-order working-set
+ * selection, an LRU cache of cache_columns columns, columns fetched through
+ * `columns` (with up to prefetch - 1 likely next ones while the cache has
+ * room).  coef [n] = y_t alpha_t, bias = -rho (score = K coef + bias).
+ * Replaces csmo_solve (_csmo.c:186) and _smo_csolver (solver.py:260-392). */
+int gkm_smo_solve(int32_t n, int32_t N, const double *y, const double *p, const double *diag,
+                  double C_pos, double C_neg, double tol, int64_t max_iter, int32_t cache_columns,
+                  int32_t prefetch, gkm_columns_cb columns, void *ctx, double *coef, double *bias,
+                  int64_t *iterations, int32_t verbose);
+
 #ifdef __cplusplus
 }
 #endif
