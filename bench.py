@@ -44,8 +44,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--queries", type=int, default=100000)
     ap.add_argument("--no-extras", action="store_true", help="skip t=2, plain-call and CPU legs")
-    ap.add_argument("--leg", default="all", choices=["all", "gram"],
-                    help="gram: run only the Gram-matrix leg (one GPU) and print its JSON")
+    ap.add_argument("--leg", default="all", choices=["all", "gram", "train"],
+                    help="gram / train: run only the Gram-matrix or the SMO training leg (one GPU), print its JSON")
     ap.add_argument("--gram-n", type=int, default=4000, help="sequences of the Gram-matrix leg")
     return ap.parse_args()
 
@@ -365,6 +365,41 @@ def gram_leg(n=4000, forms=("index", "dense", "join")):
     return out
 
 
+def training_leg(n=4000, seed=5):
+    """SMO C-SVC training (the reference's column-cached solver) on the config-2
+    sequences (n, 100..1,000 bp log-uniform), t=4 wgkm l=11 k=7 d=3, C=1,
+    tol=1e-3: a fixed 10 bp motif planted at a random position in half of the
+    sequences makes the positive class.  Columns from the GPU l-mer index,
+    solver on the host."""
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+    import gkmsvm_lite_b200.synthetic as syn
+    from gkmsvm_lite_b200.solver import last_solve_stats
+
+    x, xl = syn.config2(n=n)
+    rng = np.random.default_rng(seed)
+    motif = rng.integers(0, 4, 10).astype(np.uint8)
+    y = np.where(rng.random(n) < 0.5, 1.0, -1.0)
+    for i in np.flatnonzero(y > 0):
+        p = rng.integers(0, max(1, int(xl[i]) - 10))
+        x[i, p:p + 10] = motif
+    k = gk.CenterWeightedGkmKernel(11, 7, d=3)
+    gk.smo_solve(k, x[:64], y[:64], lengths=xl[:64])  # warm-up: library, graphs, allocator
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    coef, bias = gk.smo_solve(k, x, y, C=1.0, tol=1e-3, lengths=xl)
+    dt = time.perf_counter() - t0
+    st = last_solve_stats()
+    # training accuracy from the Gram matrix (outside the timed region)
+    acc = float((np.sign(gk.compute_gram(k, x, lengths=xl) @ coef + bias) == y).mean())
+    return {"workload": f"config2 sequences: {n} x 100-1000 bp, t=4 wgkm l=11 k=7 d=3, C=1, tol=1e-3, "
+                        "planted-motif labels",
+            "train_s": dt, "iterations": st.get("iterations"), "column_calls": st.get("calls"),
+            "columns": st.get("columns"), "support_vectors": int((np.abs(coef) > 0).sum()),
+            "train_accuracy": acc}
+
+
 def run_b200(args):
     import torch
 
@@ -539,6 +574,7 @@ def run_b200(args):
                 result["serving"] = serving_leg(sv, svl, coef)
                 result["ism_explain"] = ism_explain_leg(sv, svl, coef)
                 result["gram"] = gram_leg(args.gram_n)
+                result["training"] = training_leg(args.gram_n)
                 result["cpu_baseline"] = cpu_baseline((sv, svl, coef), model._sv_diag().cpu().numpy(), xq, xl,
                                                       PARAMS_T3)
     if rank == 0:
@@ -556,6 +592,9 @@ def main():
         return run_reference(args)
     if args.leg == "gram":
         print(json.dumps(gram_leg(args.gram_n)), flush=True)
+        return 0
+    if args.leg == "train":
+        print(json.dumps(training_leg(args.gram_n)), flush=True)
         return 0
     return run_b200(args)
 

@@ -114,6 +114,14 @@ def _check_kernel(kernel):
         raise ValueError("smo_solve needs a normalized kernel")
 
 
+_LAST_STATS: dict = {}
+
+
+def last_solve_stats() -> dict:
+    """Iterations, column-provider calls and columns of the last solve."""
+    return dict(_LAST_STATS)
+
+
 def _solve(cache: KernelColumnCache, y, p, C, tol, max_iter, cache_size, verbose):
     N = cache.N
     y = np.ascontiguousarray(y, dtype=np.float64)
@@ -121,9 +129,12 @@ def _solve(cache: KernelColumnCache, y, p, C, tol, max_iter, cache_size, verbose
     n = y.shape[0]
     diag = np.ascontiguousarray(cache.finished_diagonal(), dtype=np.float64)
     errors: list[BaseException] = []
+    stats = {"calls": 0, "columns": 0}
 
     def provider(count, idx_ptr, out_ptr, ctx):
         try:
+            stats["calls"] += 1
+            stats["columns"] += count
             idx = np.ctypeslib.as_array(idx_ptr, shape=(count,)).copy()
             cols = cache.device_columns(idx).cpu().numpy()
             out = np.ctypeslib.as_array(out_ptr, shape=(count * N,))
@@ -144,6 +155,8 @@ def _solve(cache: KernelColumnCache, y, p, C, tol, max_iter, cache_size, verbose
     if errors:
         raise RuntimeError("SMO kernel column computation failed") from errors[0]
     _lib.check(st, "gkm_smo_solve")
+    _LAST_STATS.clear()
+    _LAST_STATS.update(stats, iterations=int(iters.value), n=n, N=N)
     return coef, float(bias.value), int(iters.value)
 
 
