@@ -44,8 +44,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--queries", type=int, default=100000)
     ap.add_argument("--no-extras", action="store_true", help="skip t=2, plain-call and CPU legs")
-    ap.add_argument("--leg", default="all", choices=["all", "gram", "train"],
-                    help="gram / train: run only the Gram-matrix or the SMO training leg (one GPU), print its JSON")
+    ap.add_argument("--leg", default="all", choices=["all", "gram", "train", "explain"],
+                    help="gram / train / explain: run only the Gram-matrix, SMO training or config-4 ISM and "
+                         "GkmExplain leg (one GPU), print its JSON")
     ap.add_argument("--gram-n", type=int, default=4000, help="sequences of the Gram-matrix leg")
     return ap.parse_args()
 
@@ -299,6 +300,20 @@ def ism_explain_leg(sv, svl, coef, n=512):
         b.record()
         torch.cuda.synchronize()
         out[name] = {"value": n / (a.elapsed_time(b) / 1e3), "unit": "seqs/sec"}
+    # the explain table's own build (1 + 4 + 4l Walsh-Hadamard transforms), V already built
+    from gkmsvm_lite_b200 import explain as ex
+
+    model._explain_tables.clear()
+    torch.cuda.synchronize()
+    a.record()
+    ex._explain_table(model, 1 << 62, False, model._device)
+    b.record()
+    torch.cuda.synchronize()
+    n_lmers = 4 ** model.kernel.base.l
+    ms = a.elapsed_time(b)
+    out["explain_table_build"] = {"ms": ms, "table_bytes": n_lmers * 4 * model.kernel.base.l * 8,
+                                  "wht_pass_bytes_total": 2 * 8 * n_lmers * (5 + 4 * model.kernel.base.l)
+                                  * model.kernel.base.l}
     out["ism_path"] = "l-mer table + fused mutant self-kernels" if model._lmer_table is not None else "index"
     out["explain_path"] = "explain table (GPU Walsh-Hadamard build, cached)" if model._explain_tables else "l-mer neighbours"
     return out
@@ -595,6 +610,11 @@ def main():
         return 0
     if args.leg == "train":
         print(json.dumps(training_leg(args.gram_n)), flush=True)
+        return 0
+    if args.leg == "explain":
+        import gkmsvm_lite_b200.synthetic as syn
+
+        print(json.dumps(ism_explain_leg(*syn.config3_model())), flush=True)
         return 0
     return run_b200(args)
 
