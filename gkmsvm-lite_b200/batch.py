@@ -182,8 +182,67 @@ class BatchedScorer:
     def check_flags(self, g=None):
         """Waits for the last batch; reruns it eagerly with 32-bit counters if
         a query block's 16-bit carries outgrew its log meanwhile (the graph
-        keeps the fast kernel)."""
+        keeps the fast kernel).  Returns True when it reran."""
         if g is None:
             g = self._last
         if self.index is not None:
-            self.index.settle(self._before, g._body)
+            return self.index.settle(self._before, g._body)
+        return False
+
+
+class DirectScorer:
+    """BatchedScorer's interface without graphs or bucket padding, for small
+    batches: the index query sees the batch's real rows, so a few long rows
+    are cut into window ranges over the whole GPU (row splits) instead of
+    keeping one SM per (row, SV tile).  Results equal model(x)'s."""
+
+    def __init__(self, model):
+        self.model = model
+        kernel = model.kernel
+        self.normalize = kernel.base.normalize
+        self.rbf = isinstance(kernel, RbfKernel)
+        self.gamma = kernel.gamma if self.rbf else 0.0
+        self.table = model._lmer_table_for()
+        self.index = None
+        if self.table is None:
+            self.index = model._sv_index()
+            if self.index is None:
+                raise ValueError("direct scoring needs the l-mer index or the l-mer table")
+        self._rerun = None
+
+    def score(self, codes: torch.Tensor, lengths: torch.Tensor | None = None, events=None,
+              check: bool = True) -> torch.Tensor:
+        m = self.model
+        spec = m._spec()
+        fwd, rc, counts = engine.pack(spec, codes, lengths)
+        if events:
+            events[0].record()
+        if self.table is not None:
+            out = engine.table_score(spec, self.table, fwd, rc, counts, m.bias, self.normalize)
+        else:
+            if self.normalize:
+                dx = engine.self_kernel(spec, fwd, rc, counts)
+                inv_dx = 1.0 / torch.sqrt(torch.clamp(dx, min=1e-20))
+            else:
+                inv_dx = torch.ones(fwd.shape[0], dtype=torch.float64, device=fwd.device)
+            out = torch.empty(fwd.shape[0], dtype=torch.float64, device=fwd.device)
+
+            def run():
+                self.index.score(fwd, counts, inv_dx, m._inv_ds(), m._sv_coef(), self.gamma, self.rbf, m.bias,
+                                 out=out, check=False)
+
+            self._before = self.index.counters()
+            run()
+            self._rerun = run
+        if events:
+            events[1].record()
+        if check:
+            self.check_flags()
+        return out
+
+    def check_flags(self, g=None):
+        """Waits for the last batch; reruns it with 32-bit counters if a query
+        block's 16-bit carries outgrew its log.  Returns True when it reran."""
+        if self.index is not None and self._rerun is not None:
+            return self.index.settle(self._before, self._rerun)
+        return False

@@ -185,10 +185,13 @@ class DeviceIndex:
         """After a call bracketed by counters() snapshots: waits for the
         stream; if a query block's 16-bit carries outgrew its log anywhere in
         that window (this call's or a concurrent one's), reruns rerun() with
-        32-bit counters (exact either way).  A wrapped 32-bit count raises."""
+        32-bit counters (exact either way).  A wrapped 32-bit count raises.
+        Returns True when it reran."""
         after = self.counters()
         torch.cuda.current_stream().synchronize()
+        reran = False
         if int(after[0]) != int(before[0]) and rerun is not None:
+            reran = True
             self.set_wide(True)
             try:
                 b2 = self.counters()
@@ -200,6 +203,7 @@ class DeviceIndex:
                 self.set_wide(False)
         if int(after[1]) != int(before[1]):
             raise _lib.GkmError(_lib.GKM_ERR_CAPACITY, "a weighted pair count passed 2^32 for one (row, SV) pair")
+        return reran
 
     def checked(self, run):
         """run() through the index, exact: see settle()."""

@@ -64,3 +64,22 @@ def test_results_same_alone_and_in_the_mix(kt):
     for r, a, b in zip(reqs, got, solo):
         np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12, err_msg=r["kind"])
     assert st["all"]["n"] == len(reqs) and st["admitted"] > 0
+
+
+@pytest.mark.parametrize("kt", ["gkmrbf", "wgkmrbf", "gkm_esttrunc"])
+def test_direct_scorer_equals_model(kt):
+    """Small serving batches skip the graphs: the same scores as model(x),
+    also when a poly-A row's 16-bit carries force the exact rerun."""
+    from gkmsvm_lite_b200.batch import DirectScorer
+
+    rng = np.random.default_rng(21)
+    sv = np.concatenate([np.zeros((6, 300), np.uint8), rng.integers(0, 4, (60, 300)).astype(np.uint8)])
+    m = gk.GkmSVM(sv, rng.normal(0, 0.1, 66), 0.1, kt, {"L": 11, "k": 7, "d": 3, "gamma": 1.0}).cuda()
+    m.use_lmer_table = False
+    x = np.concatenate([np.zeros((1, 2000), np.uint8), rng.integers(0, 4, (3, 2000)).astype(np.uint8)])
+    lengths = np.array([2000, 1500, 700, 11])
+    want = m(x, lengths=lengths).cpu().numpy()[:, 0]
+    ds = DirectScorer(m)
+    got = ds.score(torch.from_numpy(x).cuda(), torch.from_numpy(lengths).cuda(), check=False)
+    ds.check_flags()
+    np.testing.assert_allclose(got.cpu().numpy(), want, rtol=1e-12, atol=1e-14)
