@@ -142,6 +142,109 @@ __global__ void explain_gather(const double *__restrict__ part, const int32_t *_
     out[idx] = s * inv_dx[b];
 }
 
+
+// Per-SV GkmExplain (explain/cpu.py:14-66) for models the l-mer path does not
+// take (l > 12): a block per query window i of row b; its warps sweep every
+// SV window (forward, then RC, SV after SV), a lane per window, and take the
+// pairs within the cutoff (ballot) one at a time in lane order; lane k adds
+// the pair's contribution at position k to its four per-base registers.  The
+// warps' [4, l] sums are added in warp order: deterministic.
+constexpr int PX_WARPS = 8;
+
+struct PairsArgs {
+    const uint32_t *fwd;
+    const int32_t *cnt;
+    int64_t W;
+    const uint32_t *by;
+    const uint32_t *ry;
+    const int32_t *cy;
+    int64_t S;
+    int64_t Wy;
+    const double *w;  // [B, S] per-(row, SV) weight
+    int l;
+    int min_matches;
+    int weighted;
+    int include_rc;
+    const uint8_t *wd;
+    const double *ta;
+    const double *tb;
+    int perturbation;
+    double *part;  // [B, W, 4, l]
+};
+
+__global__ void __launch_bounds__(PX_WARPS * 32) explain_pairs(PairsArgs a)
+{
+    __shared__ double red[PX_WARPS][4][16];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t i = blockIdx.x, b = blockIdx.y;
+    const int n = a.cnt[b];
+    const int l = a.l;
+    double *out = a.part + ((b * a.W + i) * 4) * l;
+    if (i >= n) {  // past the row's windows: nothing
+        for (int t = threadIdx.x; t < 4 * l; t += blockDim.x) out[t] = 0.0;
+        return;
+    }
+    const uint32_t u = a.fwd[b * a.W + i];
+    const double wx = a.weighted ? (double)gkm_wt(a.wd, n, (int)i) : 1.0;
+    const int xk = lane < l ? (int)((u >> (2 * lane)) & 3u) : 0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const bool rc = a.include_rc && a.ry != nullptr;
+    for (int64_t s = warp; s < a.S; s += PX_WARPS) {
+        const double ws = a.w[b * a.S + s];
+        const int ny = a.cy[s];
+        const int nt = rc ? 2 * ny : ny;
+        if (ws == 0.0) continue;
+        for (int c0 = 0; c0 < nt; c0 += 32) {
+            const int t = c0 + lane;
+            uint32_t v = GKM_PAD;
+            double wy = 1.0;
+            if (t < nt) {
+                if (t < ny) {
+                    v = a.by[s * a.Wy + t];
+                    if (a.weighted) wy = (double)gkm_wt(a.wd, ny, t);
+                } else {  // RC of forward window ny - 1 - (t - ny)
+                    const int f = ny - 1 - (t - ny);
+                    v = a.ry[s * a.Wy + (a.Wy - 1 - f)];
+                    if (a.weighted) wy = (double)gkm_wt(a.wd, ny, f);
+                }
+            }
+            const int mm = v == GKM_PAD ? 99 : gkm_mism(u, v);
+            unsigned hits = __ballot_sync(GKM_FULL, l - mm >= a.min_matches);
+            while (hits) {
+                const int h = __ffs(hits) - 1;
+                hits &= hits - 1;
+                const uint32_t vh = __shfl_sync(GKM_FULL, v, h);
+                const int mh = __shfl_sync(GKM_FULL, mm, h);
+                const double ew = ws * wx * __shfl_sync(GKM_FULL, wy, h);
+                if (lane < l) {
+                    const int yk = (int)((vh >> (2 * lane)) & 3u);
+                    const double av = ew * a.ta[mh], bv = ew * a.tb[mh];
+                    if (!a.perturbation) {
+                        const double val = xk == yk ? av : bv;
+#pragma unroll
+                        for (int d = 0; d < 4; d++) acc[d] += d == yk ? val : 0.0;
+                    } else if (xk == yk) {
+#pragma unroll
+                        for (int d = 0; d < 4; d++) acc[d] += d != yk ? av : 0.0;
+                    } else {
+#pragma unroll
+                        for (int d = 0; d < 4; d++) acc[d] += d == yk ? bv : 0.0;
+                    }
+                }
+            }
+        }
+    }
+    if (lane < l)
+        for (int d = 0; d < 4; d++) red[warp][d][lane] = acc[d];
+    __syncthreads();
+    for (int t = threadIdx.x; t < 4 * l; t += blockDim.x) {
+        const int d = t / l, k = t - d * l;
+        double sum = 0.0;
+        for (int q = 0; q < PX_WARPS; q++) sum += red[q][d][k];
+        out[d * l + k] = sum;  // base d at position i + k
+    }
+}
+
 }  // namespace
 
 extern "C" int gkm_explain_lmer(const gkm_spec *spec, const uint32_t *fwd, const int32_t *counts, int64_t B,
@@ -189,6 +292,55 @@ extern "C" int gkm_explain_lmer(const gkm_spec *spec, const uint32_t *fwd, const
     int s = GKM_OK;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) s = gkm_cuda_status(e, "explain_windows");
+    if (s == GKM_OK) {
+        int64_t n = B * 4 * L;
+        explain_gather<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, counts, B, W, L, spec->l, inv_dx, out);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) s = gkm_cuda_status(e, "explain_gather");
+    }
+    cudaFreeAsync(part, st);
+    return s;
+}
+
+extern "C" int gkm_explain_pairs(const gkm_spec *spec, const uint32_t *fwd, const int32_t *counts, int64_t B,
+                                 int64_t W, int64_t L, const double *inv_dx, const uint32_t *by, const uint32_t *ry,
+                                 const int32_t *cy, int64_t S, int64_t Wy, const double *w, const double *table_a,
+                                 const double *table_b, int32_t min_matches, int32_t perturbation, double *out,
+                                 gkm_stream_t stream)
+{
+    if (!spec || !fwd || !counts || !inv_dx || !by || !cy || !w || !table_a || !table_b || !out)
+        return gkm_fail(GKM_ERR_INVALID, "null argument");
+    if (spec->l < 1 || spec->l > 15) return gkm_fail(GKM_ERR_INVALID, "l must be in 1..15");
+    if (spec->weighted && (!spec->wd || spec->wd_len < 1)) return gkm_fail(GKM_ERR_INVALID, "weighted spec without weights");
+    if (B == 0 || W == 0 || L == 0) return GKM_OK;
+    if (B > 65535 || W > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many rows or windows per launch");
+    cudaStream_t st = (cudaStream_t)stream;
+    double *part = nullptr;
+    if (cudaMallocAsync(&part, sizeof(double) * B * W * 4 * spec->l, st) != cudaSuccess)
+        return gkm_fail(GKM_ERR_OOM, "explain scratch");
+    PairsArgs a = {};
+    a.fwd = fwd;
+    a.cnt = counts;
+    a.W = W;
+    a.by = by;
+    a.ry = ry;
+    a.cy = cy;
+    a.S = S;
+    a.Wy = Wy;
+    a.w = w;
+    a.l = spec->l;
+    a.min_matches = min_matches;
+    a.weighted = spec->weighted;
+    a.include_rc = spec->include_rc;
+    a.wd = spec->wd;
+    a.ta = table_a;
+    a.tb = table_b;
+    a.perturbation = perturbation;
+    a.part = part;
+    explain_pairs<<<dim3((unsigned)W, (unsigned)B), PX_WARPS * 32, 0, st>>>(a);
+    int s = GKM_OK;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) s = gkm_cuda_status(e, "explain_pairs");
     if (s == GKM_OK) {
         int64_t n = B * 4 * L;
         explain_gather<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, counts, B, W, L, spec->l, inv_dx, out);

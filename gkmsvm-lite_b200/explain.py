@@ -24,7 +24,7 @@ from . import engine
 from ._lib import call, ptr, stream_handle
 from .inputs import (allele_arrays, as_batch, device_codes, joint_lengths, nan_rows, per_position, rows,
                      short_rows)
-from .kernels import RbfKernel, explain_tables, neighbor_masks
+from .kernels import INDEX_MAX_L, MAX_NEIGHBORS, RbfKernel, explain_tables, neighbor_count, neighbor_masks
 
 _MODE_ALIASES = {0: "importance", 1: "hypothetical", 2: "perturbation", "importance": "importance",
                  "hypothetical": "hypothetical", "perturbation": "perturbation"}
@@ -66,6 +66,40 @@ def _explain_V(model) -> torch.Tensor:
         if tmp is not None:
             tmp.close()
     return c["explain_V"]
+
+
+# SV windows a query window visits per l-mer neighbour before the per-SV pair
+# loop is the cheaper form (explain/lmer.py:25)
+_EXPLAIN_SV_WINDOWS_PER_NEIGHBOR = 6
+
+
+def _explain_uses_pairs(model, perturbation: bool) -> bool:
+    """Whether attributions go through the per-SV pair loop
+    (explain/core.py:170-247) because the l-mer path does not apply
+    (explain/lmer.py:60-85): the index is off, l > 12, no pair contributes,
+    the neighbourhood outweighs the SV windows, or an RBF model has no index."""
+    base = model.kernel.base
+    _, _, dmax = explain_tables(base, perturbation)
+    if not model.use_lmer_index or base.l > INDEX_MAX_L or dmax < 0:
+        return True
+    n = neighbor_count(base.l, dmax)
+    if n > MAX_NEIGHBORS:
+        fwd, rc, _ = model._sv_packed()
+        sv_windows = fwd.numel() + (0 if rc is None else rc.numel())
+        if n * _EXPLAIN_SV_WINDOWS_PER_NEIGHBOR > sv_windows:
+            return True
+    return isinstance(model.kernel, RbfKernel) and model._sv_index() is None
+
+
+def _explain_pair_tables(model, perturbation: bool, dev):
+    """Device (table_a, table_b) and the minimum matches of a contributing pair."""
+    base = model.kernel.base
+    key = ("explain_pair_tables", perturbation)
+    c = model._sv_cache
+    if key not in c:
+        a, b, dmax = explain_tables(base, perturbation)
+        c[key] = (torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev), base.l - dmax)
+    return c[key]
 
 
 # explain table limits and cost model ("auto"): build cost per entry of 4^l x l
@@ -138,22 +172,21 @@ def _explain_rows(model, x, lengths, mode, dev, table=None):
     fwd, rc, counts = engine.pack(spec, xt, lengths)
     spec.check_rows(int(fwd.shape[1]))
     perturbation = mode == "perturbation"
-    masks, ta, tb = _explain_masks(model, perturbation, dev)
     B, W = fwd.shape
     if base.normalize:
         dx = engine.self_kernel(spec, fwd, rc, counts)
         inv_dx = 1.0 / torch.sqrt(torch.clamp(dx, min=1e-20))
     else:
         inv_dx = torch.ones(B, dtype=torch.float64, device=dev)
-    V = index = w = None
-    if table is not None:
+    V = index = w = out = None
+    if table is None and _explain_uses_pairs(model, perturbation):
+        out = _explain_pairs(model, spec, fwd, counts, inv_dx, L, perturbation, dev)
+    elif table is not None:
         out = torch.empty((B, 4, L), dtype=torch.float64, device=dev)
         call("gkm_explain_table", spec.ref, ptr(table), ptr(fwd), ptr(counts), B, W, L, ptr(inv_dx),
              int(perturbation), ptr(out), stream_handle())
     elif isinstance(kernel, RbfKernel):
-        index = model._sv_index()
-        if index is None:
-            raise NotImplementedError("RBF GkmExplain needs the l-mer index")
+        index = model._sv_index()  # not None: _explain_uses_pairs
         raw, _ = index.pairwise(fwd, counts)
         inv_ds = model._inv_ds()
         k_norm = raw * inv_dx[:, None] * inv_ds[None, :]
@@ -161,7 +194,8 @@ def _explain_rows(model, x, lengths, mode, dev, table=None):
         w = w.contiguous()
     else:
         V = _explain_V(model)
-    if table is None:
+    if table is None and out is None:
+        masks, ta, tb = _explain_masks(model, perturbation, dev)
         out = torch.empty((B, 4, L), dtype=torch.float64, device=dev)
         call("gkm_explain_lmer", spec.ref, ptr(fwd), ptr(counts), B, W, L, ptr(inv_dx), ptr(V),
              None if index is None else index.handle, ptr(w), ptr(masks), int(masks.numel()), ptr(ta), ptr(tb),
@@ -169,6 +203,27 @@ def _explain_rows(model, x, lengths, mode, dev, table=None):
     if mode == "importance":
         oh = torch.nn.functional.one_hot(xt.long(), 4).permute(0, 2, 1).to(out.dtype)
         out = out * oh
+    return out
+
+
+def _explain_pairs(model, spec, fwd, counts, inv_dx, L: int, perturbation: bool, dev) -> torch.Tensor:
+    """[B, 4, L] attributions by the per-SV pair loop (gkm_explain_pairs):
+    per-(row, SV) weights coef_s / sqrt(K(sv, sv)), RBF-scaled by the row's
+    normalised kernel value with each SV (explain/core.py:207-226)."""
+    kernel = model.kernel
+    by, ry, cy = model._sv_packed()
+    inv_ds = model._inv_ds()
+    B, W = fwd.shape
+    S = int(by.shape[0])
+    w = (model._sv_coef() * inv_ds)[None, :].expand(B, S)
+    if isinstance(kernel, RbfKernel):
+        raw, _ = engine.pairwise(spec, fwd, counts, by, ry, cy)
+        w = w * _rbf_scale(raw * inv_dx[:, None] * inv_ds[None, :], kernel.gamma)
+    w = w.contiguous()
+    ta, tb, min_matches = _explain_pair_tables(model, perturbation, dev)
+    out = torch.empty((B, 4, L), dtype=torch.float64, device=dev)
+    call("gkm_explain_pairs", spec.ref, ptr(fwd), ptr(counts), B, W, L, ptr(inv_dx), ptr(by), ptr(ry), ptr(cy), S,
+         int(by.shape[1]), ptr(w), ptr(ta), ptr(tb), int(min_matches), int(perturbation), ptr(out), stream_handle())
     return out
 
 

@@ -229,6 +229,23 @@ int gkm_explain_lmer(const gkm_spec *spec, const uint32_t *fwd, const int32_t *c
                      const double *table_b, int32_t perturbation, double *out,
                      gkm_stream_t stream);
 
+/* GkmExplain by the per-SV pair loop, for models the l-mer path does not take
+ * (l > 12, a neighbourhood larger than the SVs, no l-mer index): every query
+ * window against every SV window by (SV s) forward and, with include_rc, RC
+ * (by / ry [S, Wy] from gkm_pack, cy [S] their counts); a pair with at least
+ * min_matches matching positions adds a(m) or b(m) times w[b, s] (and the two
+ * window weights when weighted) to each position.  w [B, S]: coef_s /
+ * sqrt(K(sv_s, sv_s)), times the RBF scale of K(x_b, sv_s) for RBF models;
+ * inv_dx [B] scales each row.  out [B, 4, L]; deterministic.
+ * Replaces _explain_cpu / _explain_gpu (explain/cpu.py:14-66,
+ * explain/core.py:170-247). */
+int gkm_explain_pairs(const gkm_spec *spec, const uint32_t *fwd, const int32_t *counts,
+                      int64_t B, int64_t W, int64_t L, const double *inv_dx,
+                      const uint32_t *by, const uint32_t *ry, const int32_t *cy,
+                      int64_t S, int64_t Wy, const double *w, const double *table_a,
+                      const double *table_b, int32_t min_matches, int32_t perturbation,
+                      double *out, gkm_stream_t stream);
+
 /* The GkmExplain table of a linear model: A [4^l, 4, l] float64 (caller
  * allocates, 1.5 GB at l = 11), every l-mer's attribution, from V [4^l] and
  * the level tables table_a / table_b [l + 2] (device), by radix-4
