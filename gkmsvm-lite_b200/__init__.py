@@ -3,6 +3,7 @@ kernel path: GkmSVM scoring, score_variants, ISM, GkmExplain, the training
 Gram matrix and the SMO solver's kernel columns, with the reference's signatures, computed by hand-written CUDA
 kernels behind the C ABI of include/gkm_b200.h."""
 
+from .deltasvm import DeltaSVMWeights, deltasvm_weights
 from .explain import gkmexplain, mutation_impact
 from .gram import compute_gram
 from .importers import load_lsgkm_model, load_model
@@ -19,5 +20,5 @@ __all__ = [
     "KERNEL_ALIASES", "KERNEL_BUILDERS", "resolve_kernel_type", "GkmKernel", "DirectGkmKernel",
     "EstTruncGkmKernel", "CenterWeightedGkmKernel", "RbfKernel", "RbfGkmKernel",
     "CenterWeightedRbfGkmKernel", "as_batch", "encode_codes", "to_codes", "KernelColumnCache", "smo_solve",
-    "smo_svr_solve",
+    "smo_svr_solve", "DeltaSVMWeights", "deltasvm_weights",
 ]

@@ -66,6 +66,7 @@ SIGNATURES = {
     "gkm_index_count": [P, P, P, I64, I64, P, P],
     "gkm_index_score_noalloc": [P, P, P, I64, I64, P, P, P, D, I32, D, P, P, P],
     "gkm_lmer_table": [SPEC, P, P, I32, P, P],
+    "gkm_deltasvm_table": [SPEC, P, D, I32, P, P],
     "gkm_table_score": [SPEC, P, P, P, P, I64, I64, D, I32, P, P, P, P],
     "gkm_mutant_diag": [SPEC, P, P, I64, I64, I64, P, P, P],
     "gkm_ism_table": [SPEC, P, P, P, I64, I64, I64, P, P, P, I32, P, P],

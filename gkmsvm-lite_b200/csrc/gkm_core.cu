@@ -636,6 +636,43 @@ extern "C" int gkm_lmer_table(const gkm_spec *spec, const double *V, const uint3
     return GKM_OK;
 }
 
+// DeltaSVM weights read off the l-mer table (svm.py:667-704): out[idx], idx in
+// DeltaSVM order (first base most significant), = table[idx with its digits
+// reversed] times the lone window's weight, divided by sqrt(K(u, u)) of the
+// l-mer alone when qnorm (h(0), plus h(m(u, rc u)) with RC, times the weight
+// squared).
+__global__ void deltasvm_table_kernel(gkm_spec sp, const double *__restrict__ table, double wt, int qnorm,
+                                      double *__restrict__ out, int64_t n)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const int l = sp.l;
+    const uint32_t u = (uint32_t)idx;
+    uint32_t packed = 0;
+    for (int p = 0; p < l; p++) packed |= ((u >> (2 * (l - 1 - p))) & 3u) << (2 * p);
+    double w = table[packed] * wt;
+    if (qnorm) {
+        double self_k = sp.h[0];
+        if (sp.include_rc) self_k = self_k + sp.h[gkm_mism(packed, gkm_rc_word(packed, l))];
+        self_k = self_k * (wt * wt);
+        w = w / sqrt(fmax(self_k, 1e-10));
+    }
+    out[idx] = w;
+}
+
+extern "C" int gkm_deltasvm_table(const gkm_spec *spec, const double *table, double window_weight,
+                                  int32_t query_norm, double *out, gkm_stream_t stream)
+{
+    GKM_TRY(check_spec(spec));
+    if (!table || !out) return gkm_fail(GKM_ERR_INVALID, "null table or out");
+    if (spec->l > 12) return gkm_fail(GKM_ERR_UNSUPPORTED, "l-mer tables need l <= 12");
+    int64_t n = (int64_t)1 << (2 * spec->l);
+    deltasvm_table_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*spec, table, window_weight,
+                                                                                        query_norm, out, n);
+    GKM_CHECK_LAUNCH("deltasvm_table");
+    return GKM_OK;
+}
+
 static int mutant_launch(const gkm_spec *spec, const uint32_t *fwd, const int32_t *counts, int64_t B,
                          int64_t W, int64_t L, const double *diag, double *mut_diag, const double *table,
                          const double *ref_raw, int normalize, double *out, cudaStream_t st)

@@ -124,9 +124,10 @@ __global__ void __launch_bounds__(EX_WARPS * 32) explain_windows(ExplainArgs a)
 }
 
 // out[b, base, p] = inv_dx[b] * sum over windows i covering p of part[b, i, base, p - i]
+// (nsplit > 1: part is [nsplit, B, W, 4, l], the splits added in order)
 __global__ void explain_gather(const double *__restrict__ part, const int32_t *__restrict__ cnt, int64_t B,
                                int64_t W, int64_t L, int l, const double *__restrict__ inv_dx,
-                               double *__restrict__ out)
+                               double *__restrict__ out, int nsplit = 1)
 {
     int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= B * 4 * L) return;
@@ -138,110 +139,130 @@ __global__ void explain_gather(const double *__restrict__ part, const int32_t *_
     int64_t i0 = p - l + 1 > 0 ? p - l + 1 : 0;
     int64_t i1 = p < n - 1 ? p : n - 1;
     double s = 0.0;
-    for (int64_t i = i0; i <= i1; i++) s += part[((b * W + i) * 4 + base) * l + (p - i)];
+    const int64_t zs = B * W * 4 * l;
+    for (int64_t i = i0; i <= i1; i++)
+        for (int z = 0; z < nsplit; z++) s += part[z * zs + ((b * W + i) * 4 + base) * l + (p - i)];
     out[idx] = s * inv_dx[b];
 }
 
 
 // Per-SV GkmExplain (explain/cpu.py:14-66) for models the l-mer path does not
-// take (l > 12): a block per query window i of row b; its warps sweep every
-// SV window (forward, then RC, SV after SV), a lane per window, and take the
-// pairs within the cutoff (ballot) one at a time in lane order; lane k adds
-// the pair's contribution at position k to its four per-base registers.  The
-// warps' [4, l] sums are added in warp order: deterministic.
+// take (l > 12, ...).  A block owns a tile of PX_QT query windows of row b and
+// a range of SVs (split z of PX splits); its warps form PX_G groups that take
+// the range's SVs in turn, and within a group each warp owns PX_QPW of the
+// tile's windows.  A warp loads 32 SV windows (forward, then RC), one a lane,
+// and tests each against its PX_QPW query windows (XOR + popcount + ballot):
+// one load serves PX_QPW tests.  Pairs within the cutoff are rare and taken one
+// at a time in lane order; lane k adds the pair's contribution at position k
+// to the query's [4, l] sums in shared memory (each address has one writer in
+// a group).  The groups' sums are added in group order and the splits in split
+// order by the gather: deterministic for a given SV count.
+constexpr int PX_QT = 32;
+constexpr int PX_G = 2;
 constexpr int PX_WARPS = 8;
+constexpr int PX_QPW = PX_QT * PX_G / PX_WARPS;
+constexpr int PX_LMAX = 16;
+static_assert(PX_WARPS % PX_G == 0 && (PX_WARPS / PX_G) * PX_QPW == PX_QT, "tile split");
 
 struct PairsArgs {
     const uint32_t *fwd;
     const int32_t *cnt;
+    int64_t B;
     int64_t W;
     const uint32_t *by;
     const uint32_t *ry;
     const int32_t *cy;
     int64_t S;
     int64_t Wy;
+    int nsplit;
     const double *w;  // [B, S] per-(row, SV) weight
     int l;
     int min_matches;
     int weighted;
-    int include_rc;
     const uint8_t *wd;
     const double *ta;
     const double *tb;
     int perturbation;
-    double *part;  // [B, W, 4, l]
+    double *part;  // [nsplit, B, W, 4, l]
 };
 
 __global__ void __launch_bounds__(PX_WARPS * 32) explain_pairs(PairsArgs a)
 {
-    __shared__ double red[PX_WARPS][4][16];
+    __shared__ double acc[PX_G][PX_QT][4][PX_LMAX];
+    __shared__ double wxs[PX_QT];
+    __shared__ uint32_t us[PX_QT];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t i = blockIdx.x, b = blockIdx.y;
+    const int64_t b = blockIdx.y;
+    const int64_t i0 = (int64_t)blockIdx.x * PX_QT;
     const int n = a.cnt[b];
+    if (i0 >= n) return;  // the gather reads windows < n only
     const int l = a.l;
-    double *out = a.part + ((b * a.W + i) * 4) * l;
-    if (i >= n) {  // past the row's windows: nothing
-        for (int t = threadIdx.x; t < 4 * l; t += blockDim.x) out[t] = 0.0;
-        return;
+    const int nq = (int)(n - i0 < PX_QT ? n - i0 : PX_QT);
+    for (int t = threadIdx.x; t < PX_G * PX_QT * 4 * PX_LMAX; t += blockDim.x) (&acc[0][0][0][0])[t] = 0.0;
+    for (int q = threadIdx.x; q < PX_QT; q += blockDim.x) {
+        us[q] = q < nq ? a.fwd[b * a.W + i0 + q] : 0u;
+        wxs[q] = q < nq && a.weighted ? (double)gkm_wt(a.wd, n, (int)(i0 + q)) : 1.0;
     }
-    const uint32_t u = a.fwd[b * a.W + i];
-    const double wx = a.weighted ? (double)gkm_wt(a.wd, n, (int)i) : 1.0;
-    const int xk = lane < l ? (int)((u >> (2 * lane)) & 3u) : 0;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const bool rc = a.include_rc && a.ry != nullptr;
-    for (int64_t s = warp; s < a.S; s += PX_WARPS) {
+    __syncthreads();
+    const int g = warp / (PX_WARPS / PX_G);
+    const int q0 = (warp % (PX_WARPS / PX_G)) * PX_QPW;
+    const int mq = nq - q0 < PX_QPW ? (nq - q0 > 0 ? nq - q0 : 0) : PX_QPW;  // this warp's live windows
+    uint32_t u[PX_QPW];
+#pragma unroll
+    for (int j = 0; j < PX_QPW; j++) u[j] = us[q0 + j];
+    const int64_t z = blockIdx.z;
+    const int64_t s0 = z * a.S / a.nsplit, s1 = (z + 1) * a.S / a.nsplit;
+    const bool rc = a.ry != nullptr;
+    for (int64_t s = s0 + g; s < s1 && mq > 0; s += PX_G) {
         const double ws = a.w[b * a.S + s];
+        if (ws == 0.0) continue;
         const int ny = a.cy[s];
         const int nt = rc ? 2 * ny : ny;
-        if (ws == 0.0) continue;
+        const uint32_t *fy = a.by + s * a.Wy;
+        const uint32_t *ry = rc ? a.ry + s * a.Wy + (a.Wy - ny) : nullptr;  // RC of forward ny-1-r at r
         for (int c0 = 0; c0 < nt; c0 += 32) {
             const int t = c0 + lane;
-            uint32_t v = GKM_PAD;
-            double wy = 1.0;
-            if (t < nt) {
-                if (t < ny) {
-                    v = a.by[s * a.Wy + t];
-                    if (a.weighted) wy = (double)gkm_wt(a.wd, ny, t);
-                } else {  // RC of forward window ny - 1 - (t - ny)
-                    const int f = ny - 1 - (t - ny);
-                    v = a.ry[s * a.Wy + (a.Wy - 1 - f)];
-                    if (a.weighted) wy = (double)gkm_wt(a.wd, ny, f);
-                }
-            }
-            const int mm = v == GKM_PAD ? 99 : gkm_mism(u, v);
-            unsigned hits = __ballot_sync(GKM_FULL, l - mm >= a.min_matches);
-            while (hits) {
-                const int h = __ffs(hits) - 1;
-                hits &= hits - 1;
-                const uint32_t vh = __shfl_sync(GKM_FULL, v, h);
-                const int mh = __shfl_sync(GKM_FULL, mm, h);
-                const double ew = ws * wx * __shfl_sync(GKM_FULL, wy, h);
-                if (lane < l) {
-                    const int yk = (int)((vh >> (2 * lane)) & 3u);
-                    const double av = ew * a.ta[mh], bv = ew * a.tb[mh];
-                    if (!a.perturbation) {
-                        const double val = xk == yk ? av : bv;
+            const bool live = t < nt;
+            const uint32_t v = !live ? 0u : (t < ny ? __ldg(fy + t) : __ldg(ry + (t - ny)));
 #pragma unroll
-                        for (int d = 0; d < 4; d++) acc[d] += d == yk ? val : 0.0;
-                    } else if (xk == yk) {
+            for (int j = 0; j < PX_QPW; j++) {
+                unsigned hits = __ballot_sync(GKM_FULL, j < mq && live && l - gkm_mism(u[j], v) >= a.min_matches);
+                while (hits) {
+                    const int h = __ffs(hits) - 1;
+                    hits &= hits - 1;
+                    const uint32_t vh = __shfl_sync(GKM_FULL, v, h);
+                    const int th = c0 + h;
+                    const int mh = gkm_mism(u[j], vh);
+                    // an RC window carries its forward window's weight
+                    const double wy = a.weighted ? (double)gkm_wt(a.wd, ny, th < ny ? th : 2 * ny - 1 - th) : 1.0;
+                    const double ew = ws * wxs[q0 + j] * wy;
+                    if (lane < l) {
+                        const int xk = (int)((u[j] >> (2 * lane)) & 3u);
+                        const int yk = (int)((vh >> (2 * lane)) & 3u);
+                        double *r = &acc[g][q0 + j][0][lane];
+                        if (!a.perturbation) {
+                            r[yk * PX_LMAX] += ew * (xk == yk ? a.ta[mh] : a.tb[mh]);
+                        } else if (xk == yk) {
+                            const double av = ew * a.ta[mh];
 #pragma unroll
-                        for (int d = 0; d < 4; d++) acc[d] += d != yk ? av : 0.0;
-                    } else {
-#pragma unroll
-                        for (int d = 0; d < 4; d++) acc[d] += d == yk ? bv : 0.0;
+                            for (int d = 0; d < 4; d++)
+                                if (d != yk) r[d * PX_LMAX] += av;
+                        } else {
+                            r[yk * PX_LMAX] += ew * a.tb[mh];
+                        }
                     }
                 }
             }
         }
     }
-    if (lane < l)
-        for (int d = 0; d < 4; d++) red[warp][d][lane] = acc[d];
     __syncthreads();
-    for (int t = threadIdx.x; t < 4 * l; t += blockDim.x) {
-        const int d = t / l, k = t - d * l;
+    double *out = a.part + ((z * a.B + b) * a.W + i0) * 4 * l;
+    for (int t = threadIdx.x; t < nq * 4 * l; t += blockDim.x) {
+        const int q = t / (4 * l), r = t - q * 4 * l, d = r / l, k = r - d * l;
         double sum = 0.0;
-        for (int q = 0; q < PX_WARPS; q++) sum += red[q][d][k];
-        out[d * l + k] = sum;  // base d at position i + k
+#pragma unroll
+        for (int gg = 0; gg < PX_G; gg++) sum += acc[gg][q][d][k];
+        out[t] = sum;  // base d at position i0 + q + k
     }
 }
 
@@ -312,39 +333,51 @@ extern "C" int gkm_explain_pairs(const gkm_spec *spec, const uint32_t *fwd, cons
         return gkm_fail(GKM_ERR_INVALID, "null argument");
     if (spec->l < 1 || spec->l > 15) return gkm_fail(GKM_ERR_INVALID, "l must be in 1..15");
     if (spec->weighted && (!spec->wd || spec->wd_len < 1)) return gkm_fail(GKM_ERR_INVALID, "weighted spec without weights");
+    if (spec->include_rc && !ry) return gkm_fail(GKM_ERR_INVALID, "RC windows missing");
     if (B == 0 || W == 0 || L == 0) return GKM_OK;
-    if (B > 65535 || W > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many rows or windows per launch");
+    const int64_t tiles = (W + PX_QT - 1) / PX_QT;
+    if (B > 65535 || tiles > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many rows or windows per launch");
+    // SV splits: a fixed function of S (the summation order then does not
+    // depend on the batch), enough blocks for the GPU at small batches
+    const int nsplit = (int)(S < 1 ? 1 : (S + 31) / 32 < 16 ? (S + 31) / 32 : 16);
     cudaStream_t st = (cudaStream_t)stream;
     double *part = nullptr;
-    if (cudaMallocAsync(&part, sizeof(double) * B * W * 4 * spec->l, st) != cudaSuccess)
+    if (cudaMallocAsync(&part, sizeof(double) * nsplit * B * W * 4 * spec->l, st) != cudaSuccess)
         return gkm_fail(GKM_ERR_OOM, "explain scratch");
     PairsArgs a = {};
     a.fwd = fwd;
     a.cnt = counts;
+    a.B = B;
     a.W = W;
     a.by = by;
-    a.ry = ry;
+    a.ry = spec->include_rc ? ry : nullptr;
     a.cy = cy;
     a.S = S;
     a.Wy = Wy;
+    a.nsplit = nsplit;
     a.w = w;
     a.l = spec->l;
     a.min_matches = min_matches;
     a.weighted = spec->weighted;
-    a.include_rc = spec->include_rc;
     a.wd = spec->wd;
     a.ta = table_a;
     a.tb = table_b;
     a.perturbation = perturbation;
     a.part = part;
-    explain_pairs<<<dim3((unsigned)W, (unsigned)B), PX_WARPS * 32, 0, st>>>(a);
     int s = GKM_OK;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) s = gkm_cuda_status(e, "explain_pairs");
+    if (S > 0) {
+        explain_pairs<<<dim3((unsigned)tiles, (unsigned)B, (unsigned)nsplit), PX_WARPS * 32, 0, st>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) s = gkm_cuda_status(e, "explain_pairs");
+    } else {
+        cudaError_t e = cudaMemsetAsync(part, 0, sizeof(double) * B * W * 4 * spec->l, st);
+        if (e != cudaSuccess) s = gkm_cuda_status(e, "explain scratch");
+    }
     if (s == GKM_OK) {
         int64_t n = B * 4 * L;
-        explain_gather<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, counts, B, W, L, spec->l, inv_dx, out);
-        e = cudaGetLastError();
+        explain_gather<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, counts, B, W, L, spec->l, inv_dx, out,
+                                                                    nsplit);
+        cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) s = gkm_cuda_status(e, "explain_gather");
     }
     cudaFreeAsync(part, st);

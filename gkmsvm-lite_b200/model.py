@@ -324,3 +324,10 @@ class GkmSVM:
             return mutation_impact(self, ref, alt, ref_lengths=ref_lengths, alt_lengths=alt_lengths,
                                    batch_size=batch_size, verbose=verbose)
         raise ValueError(f"method must be 'kernel' or 'gkmexplain', got {method!r}")
+
+    def to_deltasvm(self, *, device: str = "cpu", query_norm: bool = False, verbose: bool = False):
+        """DeltaSVM weights, one per l-mer (svm.py:706-750); see
+        deltasvm.to_deltasvm."""
+        from .deltasvm import to_deltasvm
+
+        return to_deltasvm(self, device=device, query_norm=query_norm, verbose=verbose)

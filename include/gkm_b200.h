@@ -167,6 +167,13 @@ int gkm_index_lmer_weights(const gkm_index_t *index, const double *c_sv, double 
 int gkm_lmer_table(const gkm_spec *spec, const double *V, const uint32_t *masks,
                    int32_t n_masks, double *table, gkm_stream_t stream);
 
+/* DeltaSVM weights [4^l] in DeltaSVM order (first base most significant) read
+ * off the l-mer table: table[digit-reversed index] * window_weight, divided by
+ * sqrt(max(K(u, u), 1e-10)) of the l-mer alone when query_norm.
+ * Replaces _deltasvm_weights_from_table / _lmer_self_kernels (svm.py:667-704). */
+int gkm_deltasvm_table(const gkm_spec *spec, const double *table, double window_weight,
+                       int32_t query_norm, double *out, gkm_stream_t stream);
+
 /* scores[b] = sum_i wt_i table[x_i] / sqrt(max(K(x, x), 1e-10)) + bias (plain
  * sum without normalize); raw and diag (nullable) get the two parts.
  * Replaces GkmSVM._table_raw / _score_lmer_table (svm.py:559-582). */

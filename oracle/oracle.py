@@ -17,7 +17,8 @@ algorithm of the path on small inputs:
 * scores svm.py:368-451, variant scores svm.py:600-662, mutation impact
   explain/impact.py:22-48, ISM as f(mutant) - f(x) (ism.py; property checked by
   the reference's tests/test_ism.py:208-249), GkmExplain per-SV pair loop
-  explain/cpu.py:14-66 with explain/core.py:116-247, Gram gram.py:21-164.
+  explain/cpu.py:14-66 with explain/core.py:116-247, Gram gram.py:21-164,
+  DeltaSVM weights svm.py:664-785.
 
 Parity is pinned by tests/golden (outputs of gkmsvm-lite itself, generated by
 tests/golden/make_golden.py, plus LS-GKM fixtures from gkmsvm-lite's tests).
@@ -364,6 +365,29 @@ def scores(model: OracleModel, xc, xl=None) -> np.ndarray:
     if short is not None:
         out[short] = np.nan
     return out[:, None]
+
+
+def deltasvm_weights(model: OracleModel, query_norm: bool = False, idx=None) -> np.ndarray:
+    """to_deltasvm weights (svm.py:706-785) at DeltaSVM indices idx (first
+    base most significant; all 4^l when None): each l-mer scored alone, minus
+    the bias, with its own normalisation undone unless query_norm (RBF keeps
+    it).  With RC the canonical member of each l-mer/reverse-complement pair
+    is the one scored (svm.py:771-785); the table route (svm.py:667-704) is the
+    same sum read from the l-mer table."""
+    kd = model.kd
+    l = kd.l
+    powers = 4 ** np.arange(l - 1, -1, -1, dtype=np.int64)
+    idx = np.arange(4**l, dtype=np.int64) if idx is None else np.asarray(idx, dtype=np.int64)
+    digits = (idx[:, None] // powers) % 4
+    if kd.include_rc:
+        rc = ((3 - digits[:, ::-1]) * powers).sum(axis=1)
+        digits = (np.minimum(idx, rc)[:, None] // powers) % 4
+    x = np.ascontiguousarray(digits.astype(np.uint8))
+    w = scores(model, x)[:, 0] - model.bias
+    if not query_norm and kd.normalize and not kd.rbf:
+        dx = raw_from_profiles(self_profiles(x, None, kd), kd)
+        w = w * np.sqrt(np.maximum(dx, 1e-10))
+    return w
 
 
 def _joint(L, n, a, b):

@@ -8,7 +8,8 @@ groups: small (every kernel type on small ragged inputs: raw kernel values,
 self-kernels, scores, ISM, GkmExplain in three modes, variant scores, mutation
 impact, Gram), config1, config2, config3, config4, config5 (subsamples of the
 benchmark workloads), lsgkm (copies LS-GKM's gkmpredict / gkmexplain outputs
-and their models from gkmsvm-lite's test fixtures).  Inputs are regenerated in
+and their models from gkmsvm-lite's test fixtures), deltasvm (to_deltasvm
+weights of the small models).  Inputs are regenerated in
 the tests from the same seeds through gkmsvm_lite_b200.synthetic, or stored
 here when small.
 """
@@ -210,7 +211,34 @@ def lsgkm():
         f.write(f"random\t{rand_seq}\t-0.123703\n")
 
 
+DELTASVM_FULL = 4**7  # weights stored whole up to this many, else a sample
+DELTASVM_SAMPLE = 8192
+
+
+def deltasvm():
+    """to_deltasvm weights (svm.py:706-785) of the small models, with and
+    without query_norm: the whole array for l <= 7, else the weights at a
+    seeded sample of l-mers and the sum of all of them."""
+    out = {}
+    for name, kt, params, n_sv, svr, n_q, qr, seed in SMALL:
+        t0 = time.time()
+        rng = np.random.default_rng(seed)
+        sv, svl = _ragged(rng, n_sv, *svr)
+        coef = rng.normal(size=n_sv)
+        n = 4 ** params["L"]
+        idx = (np.arange(n) if n <= DELTASVM_FULL
+               else np.sort(np.random.default_rng(5).choice(n, DELTASVM_SAMPLE, replace=False)))
+        out[f"{name}/idx"] = idx
+        for key, qn in (("w", False), ("wq", True)):
+            m = GkmSVM(sv, coef, -0.15, kt, params, sv_lengths=svl)
+            w = np.asarray(m.to_deltasvm(query_norm=qn).weights, dtype=np.float64)
+            out[f"{name}/{key}"] = w[idx]
+            out[f"{name}/{key}_sum"] = w.sum()
+        print(f"deltasvm {name}: {time.time() - t0:.1f}s", flush=True)
+    np.savez_compressed(os.path.join(HERE, "deltasvm.npz"), **out)
+
+
 if __name__ == "__main__":
-    groups = sys.argv[1:] or ["small", "config1", "config2", "config3", "config4", "config5", "lsgkm"]
+    groups = sys.argv[1:] or ["small", "config1", "config2", "config3", "config4", "config5", "lsgkm", "deltasvm"]
     for g in groups:
         globals()[g]()

@@ -47,9 +47,9 @@ LONG = [
 ]
 
 
-def _long_case(seed, kernel_type, params):
+def _long_case(seed, kernel_type, params, S=24):
     rng = np.random.default_rng(seed)
-    S, Ls, B, L = 24, 70, 5, 64
+    Ls, B, L = 70, 5, 64
     sv = rng.integers(0, 4, (S, Ls), dtype=np.uint8)
     # plant shared segments so that pairs within the cutoff occur
     motif = rng.integers(0, 4, 20, dtype=np.uint8)
@@ -99,3 +99,14 @@ def test_pairs_deterministic():
     a = _np(gk.gkmexplain(m, x, lengths=x_len, mode="hypothetical"))
     b = _np(gk.gkmexplain(m, x, lengths=x_len, mode="hypothetical", batch_size=2))
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("kernel_type,params", [LONG[2], LONG[4]])
+def test_pairs_sv_splits_match_oracle(kernel_type, params):
+    """130 SVs: the SV range is split across blocks (5 splits)."""
+    sv, sv_len, coef, x, x_len = _long_case(23, kernel_type, params, S=130)
+    m = gk.GkmSVM(sv, coef, 0.0, kernel_type, params, sv_lengths=sv_len).cuda()
+    got = _np(gk.gkmexplain(m, x, lengths=x_len, mode="perturbation"))
+    kd = orc.KernelDef.from_params(kernel_type, params)
+    want = orc.gkmexplain(orc.OracleModel(sv, sv_len, coef, 0.0, kd), x, x_len, "perturbation")
+    np.testing.assert_allclose(got, want, rtol=RTOL, atol=1e-12 * np.abs(want).max())

@@ -178,3 +178,21 @@ def test_encode_10sv_gkmpredict():
         else:
             x, _ = codes_of([seq])
         assert abs(orc.scores(m, x)[0, 0] - float(want)) < 1e-4
+
+
+@pytest.fixture(scope="module")
+def deltasvm_golden():
+    z = np.load(os.path.join(GOLDEN, "deltasvm.npz"))
+    return {k: z[k] for k in z.files}
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_deltasvm_weights(small, deltasvm_golden, name):
+    """to_deltasvm weights at the fixture's l-mers, with and without query_norm."""
+    c, g = small[name], deltasvm_golden
+    m = _model(c)
+    idx = g[f"{name}/idx"]
+    for key, qn in (("w", False), ("wq", True)):
+        want = g[f"{name}/{key}"]
+        got = orc.deltasvm_weights(m, qn, idx)
+        np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-12 * max(1.0, np.abs(want).max()))
