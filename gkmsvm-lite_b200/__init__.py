@@ -6,13 +6,15 @@ kernels behind the C ABI of include/gkm_b200.h."""
 from .deltasvm import DeltaSVMWeights, deltasvm_weights
 from .explain import gkmexplain, mutation_impact
 from .gram import compute_gram
-from .importers import load_lsgkm_model, load_model
+from .importers import load_lsgkm_model, parse_lsgkm_header
 from .inputs import as_batch, encode_codes, to_codes
 from .ism import ism
 from .kernels import (KERNEL_ALIASES, KERNEL_BUILDERS, CenterWeightedGkmKernel, CenterWeightedRbfGkmKernel,
                       DirectGkmKernel, EstTruncGkmKernel, GkmKernel, RbfGkmKernel, RbfKernel,
                       resolve_kernel_type)
 from .model import GkmSVM
+from .serialization import (load_deltasvm_npz, load_model, load_npz, save_deltasvm_npz, save_lsgkm,
+                            save_npz)
 from .solver import KernelColumnCache, smo_solve, smo_svr_solve
 
 __all__ = [
@@ -20,5 +22,6 @@ __all__ = [
     "KERNEL_ALIASES", "KERNEL_BUILDERS", "resolve_kernel_type", "GkmKernel", "DirectGkmKernel",
     "EstTruncGkmKernel", "CenterWeightedGkmKernel", "RbfKernel", "RbfGkmKernel",
     "CenterWeightedRbfGkmKernel", "as_batch", "encode_codes", "to_codes", "KernelColumnCache", "smo_solve",
-    "smo_svr_solve", "DeltaSVMWeights", "deltasvm_weights",
+    "smo_svr_solve", "DeltaSVMWeights", "deltasvm_weights", "parse_lsgkm_header", "load_npz", "save_npz",
+    "save_lsgkm", "load_deltasvm_npz", "save_deltasvm_npz",
 ]

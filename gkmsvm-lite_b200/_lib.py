@@ -79,6 +79,7 @@ SIGNATURES = {
     "gkm_explain_table": [SPEC, P, P, P, I64, I64, I64, P, I32, P, P],
     "gkm_smo_solve": [I32, I32, P, P, P, D, D, D, I64, I32, I32, COLUMNS_CB, P, P, P, P, I32],
     "gkm_gram_finish": [P, I64, I64, P, P, D, I32, I32, P, P],
+    "gkm_lsgkm_parse_svs": [P, I64, I64, I64, P, P, P, P, P, P, P],
 }
 
 _lib = None

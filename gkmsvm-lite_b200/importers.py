@@ -1,76 +1,120 @@
 """LS-GKM model files (.model.txt / .model.txt.gz) -> GkmSVM, with the header
 fields and conventions of gkmsvm-lite's importers/lsgkm.py:37-97: bias = -rho,
-non-ACGT letters read as A, SVs of different lengths padded with lengths."""
+non-ACGT letters read as A, SVs of different lengths padded with lengths.  The
+SV section (nearly all of a file) is parsed and encoded natively
+(gkm_lsgkm_parse_svs); the few header lines in Python."""
 
 from __future__ import annotations
 
+import ctypes
 import gzip
+import warnings
 
 import numpy as np
 
-from .inputs import as_batch, encode_codes
+from . import _lib
+from .inputs import LSGKM_MAX_LENGTH
 from .kernels import KERNEL_ALIASES
 from .model import GkmSVM
 
 _INT = ("L", "k", "d", "M", "nr_class", "total_sv", "norc")
 _FLOAT = ("gamma", "H")
+_LIST = {"rho": float, "label": int, "nr_sv": int, "probA": float, "probB": float}
 
 
-def _open(path):
-    try:
-        f = gzip.open(path, "rt")
-        f.readline()
-        f.seek(0)
-        return f
-    except gzip.BadGzipFile:
-        return open(path)
+def _read_bytes(path) -> bytes:
+    """The file's bytes, gunzipped when it is gzip (detected by content)."""
+    with open(path, "rb") as f:
+        data = f.read()
+    if data[:2] == b"\x1f\x8b":
+        data = gzip.decompress(data)
+    return data
+
+
+def _parse_header(data: bytes) -> tuple[dict, int]:
+    """(typed header fields, offset of the SV section) of an LS-GKM file
+    (importers/__init__.py:31-50 parse_header_value)."""
+    header = {"norc": 0}
+    pos = 0
+    while pos < len(data):
+        eol = data.find(b"\n", pos)
+        if eol < 0:
+            eol = len(data)
+        line = data[pos:eol].decode("ascii", errors="replace").strip()
+        pos = eol + 1
+        if line.startswith("SV"):
+            return header, pos
+        parts = line.split(None, 1)
+        if len(parts) < 2:
+            continue
+        key, value = parts
+        if key == "kernel_type":
+            header[key] = KERNEL_ALIASES.get(int(value), value) if value.isdigit() else value
+        elif key in _INT:
+            header[key] = int(value)
+        elif key in _FLOAT:
+            header[key] = float(value)
+        elif key in _LIST:
+            header[key] = [_LIST[key](v) for v in value.split()]
+        elif key == "svm_type":
+            header[key] = value
+    return header, len(data)
+
+
+def parse_lsgkm_header(path) -> dict:
+    """Header fields of an LS-GKM model file (importers/lsgkm.py:23-34)."""
+    return _parse_header(_read_bytes(str(path)))[0]
+
+
+def parse_lsgkm_svs(text: bytes):
+    """(coefficients [n] float64, codes [n, L_max] uint8, lengths [n] int64,
+    SVs with letters other than ACGTN) of an SV section, parsed natively
+    (gkm_lsgkm_parse_svs)."""
+    lib = _lib.load()
+    buf = ctypes.c_char_p(text)
+    n, width, other, bad = (ctypes.c_int64() for _ in range(4))
+    _lib.check(lib.gkm_lsgkm_parse_svs(buf, len(text), 0, 0, None, None, None, ctypes.byref(n),
+                                       ctypes.byref(width), None, ctypes.byref(bad)), "gkm_lsgkm_parse_svs")
+    n, width = n.value, width.value
+    coef = np.empty(n, dtype=np.float64)
+    lengths = np.empty(n, dtype=np.int64)
+    codes = np.empty((n, width), dtype=np.uint8)
+    got, longest = ctypes.c_int64(), ctypes.c_int64()
+    if n:
+        _lib.check(lib.gkm_lsgkm_parse_svs(buf, len(text), n, width, coef.ctypes.data, lengths.ctypes.data,
+                                           codes.ctypes.data, ctypes.byref(got), ctypes.byref(longest),
+                                           ctypes.byref(other), ctypes.byref(bad)), "gkm_lsgkm_parse_svs")
+    return coef, codes, lengths, other.value
 
 
 def load_lsgkm_model(path, *, sv_chunk_size=None, device="cpu") -> GkmSVM:
-    header = {"norc": 0}
-    coefs, seqs = [], []
-    in_sv = False
-    with _open(str(path)) as f:
-        for line in f:
-            line = line.strip()
-            if not line:
-                continue
-            if line.startswith("SV"):
-                in_sv = True
-                continue
-            parts = line.split()
-            if not in_sv:
-                if len(parts) < 2:
-                    continue
-                key, val = parts[0], parts[1:]
-                if key == "kernel_type":
-                    header[key] = KERNEL_ALIASES.get(int(val[0]), val[0]) if val[0].isdigit() else val[0]
-                elif key in _INT:
-                    header[key] = int(val[0])
-                elif key in _FLOAT:
-                    header[key] = float(val[0])
-                elif key == "rho":
-                    header[key] = [float(v) for v in val]
-                continue
-            if len(parts) < 2:
-                raise ValueError(f"Malformed SV line: {line[:80]}")
-            coefs.append(float(parts[0]))
-            seqs.append(parts[1])
+    """GkmSVM of an LS-GKM model file, plain or gzip (importers/lsgkm.py:37-97):
+    bias = -rho; SVs of different lengths padded, with sv_lengths; letters
+    other than ACGTN read as N, with a warning."""
+    data = _read_bytes(str(path))
+    header, start = _parse_header(data)
     for key in ("kernel_type", "total_sv", "rho"):
-        if key not in header:
+        if header.get(key) is None:
             raise ValueError(f"Model file missing {key} field")
     if header.get("nr_class", 2) != 2:
-        raise NotImplementedError("Only binary classification (nr_class=2) is supported")
-    if len(seqs) != header["total_sv"]:
-        raise ValueError(f"Expected {header['total_sv']} support vectors, got {len(seqs)}")
-    codes = [encode_codes(s, allow_n=True, allow_other=True) for s in seqs]
-    sv, sv_lengths = as_batch(codes)
+        raise NotImplementedError(
+            f"Only binary classification (nr_class=2) is supported, got {header.get('nr_class')}")
+    coef, sv, lengths, other = parse_lsgkm_svs(data[start:])
+    if len(coef) == 0:
+        raise ValueError("No support vector sequences found")
+    if len(coef) != header["total_sv"]:
+        raise ValueError(f"Expected {header['total_sv']} support vectors, got {len(coef)}")
+    if other:
+        warnings.warn(f"{other} support vectors contain letters other than ACGTN; "
+                      "reading them as N (scored as A, as LS-GKM does)", stacklevel=2)
+    longest = int(lengths.max())
+    if longest > LSGKM_MAX_LENGTH:
+        warnings.warn(f"sequences up to {longest} bp: LS-GKM reads only the first "
+                      f"{LSGKM_MAX_LENGTH} bases of longer ones", stacklevel=2)
     params = {"L": header["L"], "k": header["k"], "include_rc": header.get("norc", 0) == 0}
     for key in ("d", "gamma", "M", "H"):
         if key in header:
             params[key] = header[key]
-    return GkmSVM(sv, np.array(coefs, dtype=np.float64), -header["rho"][0], header["kernel_type"], params,
-                  sv_lengths=sv_lengths, sv_chunk_size=sv_chunk_size, device=device)
-
-
-load_model = load_lsgkm_model
+    return GkmSVM(sv, coef, -header["rho"][0], header["kernel_type"], params,
+                  sv_lengths=None if (lengths == longest).all() else lengths, sv_chunk_size=sv_chunk_size,
+                  device=device)

@@ -331,3 +331,17 @@ class GkmSVM:
         from .deltasvm import to_deltasvm
 
         return to_deltasvm(self, device=device, query_norm=query_norm, verbose=verbose)
+
+    def save(self, path: str, *, fmt: str | None = None) -> None:
+        """Save to disk (svm.py:273-298): "npz" (native) or "lsgkm" (text,
+        gzip for .gz), from the extension unless fmt is given."""
+        from .serialization import save_lsgkm, save_npz
+
+        if fmt is None:
+            fmt = "npz" if str(path).lower().endswith(".npz") else "lsgkm"
+        if fmt == "npz":
+            save_npz(self, path)
+        elif fmt == "lsgkm":
+            save_lsgkm(self, path)
+        else:
+            raise ValueError(f"Unknown format {fmt!r}. Use 'npz' or 'lsgkm'.")

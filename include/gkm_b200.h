@@ -276,6 +276,21 @@ int gkm_gram_finish(const double *raw, int64_t N, int64_t M, const double *dx,
                     const double *dy, double gamma, int32_t rbf, int32_t symmetric,
                     double *out, gkm_stream_t stream);
 
+/* Host: the support-vector section of an LS-GKM model file (the text after
+ * its "SV" line), lines "<coefficient> <sequence>", blank lines skipped.  With
+ * codes NULL, counts: *n_sv lines and *max_len, the longest sequence.  Else
+ * fills coef [n], lengths [n] and codes [capacity, width] (A C G T = 0..3,
+ * lower case too; N and other letters stored as 0, zero padded) and sets
+ * *n_other, the SVs holding letters other than ACGTN.  A line with fewer than
+ * two fields, a coefficient strtod does not read whole, or a non-ASCII byte
+ * fails with GKM_ERR_INVALID and its line number within the section in
+ * *bad_line (nullable).
+ * Replaces the SV loop of load_lsgkm_model and build_model's encoding
+ * (importers/lsgkm.py:68-85, importers/__init__.py:53-113). */
+int gkm_lsgkm_parse_svs(const char *text, int64_t len, int64_t capacity, int64_t width,
+                        double *coef, int64_t *lengths, uint8_t *codes, int64_t *n_sv,
+                        int64_t *max_len, int64_t *n_other, int64_t *bad_line);
+
 /* Kernel-column provider of gkm_smo_solve: writes, for k < count, column
  * idx[k] of the normalized kernel (K(:, idx[k]), N doubles, HOST memory) to
  * out[k * N ...]; returns 0, or non-zero to stop the solver. */
