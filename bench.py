@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--queries", type=int, default=100000)
     ap.add_argument("--no-extras", action="store_true", help="skip t=2, plain-call and CPU legs")
-    ap.add_argument("--leg", default="all", choices=["all", "gram", "train", "explain"],
+    ap.add_argument("--leg", default="all", choices=["all", "gram", "train", "explain", "explain-pairs"],
                     help="gram / train / explain: run only the Gram-matrix, SMO training or config-4 ISM and "
                          "GkmExplain leg (one GPU), print its JSON")
     ap.add_argument("--gram-n", type=int, default=4000, help="sequences of the Gram-matrix leg")
@@ -322,9 +322,75 @@ def ism_explain_leg(sv, svl, coef, n=512):
     out["explain_table_build"] = {"ms": ms, "table_bytes": n_lmers * 4 * model.kernel.base.l * 8,
                                   "wht_pass_bytes_total": 2 * 8 * n_lmers * (5 + 4 * model.kernel.base.l)
                                   * model.kernel.base.l}
+    # the per-SV pair loop (gkm_explain_pairs) on the same model and rows, the
+    # form models the l-mer path does not take use (l > 12, no index)
+    nps = 16
+    model.use_lmer_index = False
+    model.use_explain_table = False
+    gk.gkmexplain(model, x[:2], mode="hypothetical")
+    torch.cuda.synchronize()
+    a.record()
+    gk.gkmexplain(model, x[:nps], mode="hypothetical", batch_size=nps)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    fw, _, cy = model._sv_packed()
+    pairs = nps * (x.shape[1] - model.kernel.base.l + 1) * int(cy.sum().item()) * 2
+    out["explain_per_sv"] = {"value": nps / (ms / 1e3), "unit": "seqs/sec", "rows": nps,
+                             "window_pairs_per_s": pairs / (ms / 1e3)}
+    model.use_lmer_index = True
+    model.use_explain_table = "auto"
     out["ism_path"] = "l-mer table + fused mutant self-kernels" if model._lmer_table is not None else "index"
     out["explain_path"] = "explain table (GPU Walsh-Hadamard build, cached)" if model._explain_tables else "l-mer neighbours"
     return out
+
+
+def deltasvm_leg(sv, svl, coef):
+    """to_deltasvm weights of the 72k-SV models: t=2 off the exact l-mer table
+    (built in the timed call), t=3 by scoring all 2.1M canonical 11-mers."""
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+
+    out = {}
+    for name, kt, params in (("t2_table", "gkm_esttrunc", PARAMS_T2), ("t3_scored", "gkmrbf", PARAMS_T3)):
+        model = gk.GkmSVM(sv, coef, 0.0, kt, params, sv_lengths=svl).cuda()
+        model._sv_diag()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        w = model.to_deltasvm(device="cuda").weights
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[name] = {"s": dt, "lmers_per_s": w.numel() / dt, "weights": int(w.numel())}
+        del model
+    return out
+
+
+def explain_pairs_leg(n_sv=2000, sv_len=300, rows=100, row_len=300, seed=9):
+    """GkmExplain through the per-SV pair loop on an l = 13 model (no l-mer
+    index or table exists past l = 12): n_sv random SVs, rows random queries."""
+    import numpy as np
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+
+    rng = np.random.default_rng(seed)
+    sv = rng.integers(0, 4, (n_sv, sv_len), dtype=np.uint8)
+    x = rng.integers(0, 4, (rows, row_len), dtype=np.uint8)
+    params = {"L": 13, "k": 8, "d": 3}
+    model = gk.GkmSVM(sv, rng.normal(0.0, 0.1, n_sv), 0.0, "gkm_esttrunc", params).cuda()
+    gk.gkmexplain(model, x[:2], mode="hypothetical")
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    gk.gkmexplain(model, x, mode="hypothetical", batch_size=rows)
+    b.record()
+    torch.cuda.synchronize()
+    s = a.elapsed_time(b) / 1e3
+    l = params["L"]
+    pairs = rows * (row_len - l + 1) * n_sv * 2 * (sv_len - l + 1)
+    return {"workload": f"l=13 k=8 d=3, {n_sv} SVs x {sv_len} bp, {rows} rows x {row_len} bp",
+            "value": rows / s, "unit": "seqs/sec", "window_pairs_per_s": pairs / s}
 
 
 def gram_leg(n=4000, forms=("index", "dense", "join")):
@@ -596,6 +662,7 @@ def run_b200(args):
             if world == 1:
                 result["serving"] = serving_leg(sv, svl, coef)
                 result["ism_explain"] = ism_explain_leg(sv, svl, coef)
+                result["deltasvm"] = deltasvm_leg(sv, svl, coef)
                 result["gram"] = gram_leg(args.gram_n)
                 result["training"] = training_leg(args.gram_n)
                 result["cpu_baseline"] = cpu_baseline((sv, svl, coef), model._sv_diag().cpu().numpy(), xq, xl,
@@ -619,10 +686,14 @@ def main():
     if args.leg == "train":
         print(json.dumps(training_leg(args.gram_n)), flush=True)
         return 0
+    if args.leg == "explain-pairs":
+        print(json.dumps(explain_pairs_leg()), flush=True)
+        return 0
     if args.leg == "explain":
         import gkmsvm_lite_b200.synthetic as syn
 
-        print(json.dumps(ism_explain_leg(*syn.config3_model())), flush=True)
+        sv, svl, coef = syn.config3_model()
+        print(json.dumps({**ism_explain_leg(sv, svl, coef), "deltasvm": deltasvm_leg(sv, svl, coef)}), flush=True)
         return 0
     return run_b200(args)
 

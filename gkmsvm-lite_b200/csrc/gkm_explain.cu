@@ -186,7 +186,7 @@ struct PairsArgs {
     double *part;  // [nsplit, B, W, 4, l]
 };
 
-__global__ void __launch_bounds__(PX_WARPS * 32) explain_pairs(PairsArgs a)
+__global__ void __launch_bounds__(PX_WARPS * 32, 5) explain_pairs(PairsArgs a)
 {
     __shared__ double acc[PX_G][PX_QT][4][PX_LMAX];
     __shared__ double wxs[PX_QT];
@@ -213,6 +213,7 @@ __global__ void __launch_bounds__(PX_WARPS * 32) explain_pairs(PairsArgs a)
     const int64_t z = blockIdx.z;
     const int64_t s0 = z * a.S / a.nsplit, s1 = (z + 1) * a.S / a.nsplit;
     const bool rc = a.ry != nullptr;
+    const int dmax = l - a.min_matches;  // largest mismatch count of a contributing pair
     for (int64_t s = s0 + g; s < s1 && mq > 0; s += PX_G) {
         const double ws = a.w[b * a.S + s];
         if (ws == 0.0) continue;
@@ -224,9 +225,14 @@ __global__ void __launch_bounds__(PX_WARPS * 32) explain_pairs(PairsArgs a)
             const int t = c0 + lane;
             const bool live = t < nt;
             const uint32_t v = !live ? 0u : (t < ny ? __ldg(fy + t) : __ldg(ry + (t - ny)));
+            // the lane's hits over its warp's query windows, one bit each
+            unsigned hm = 0;
+#pragma unroll
+            for (int j = 0; j < PX_QPW; j++) hm |= (unsigned)(j < mq && live && gkm_mism(u[j], v) <= dmax) << j;
+            if (!__any_sync(GKM_FULL, hm)) continue;  // the common case
 #pragma unroll
             for (int j = 0; j < PX_QPW; j++) {
-                unsigned hits = __ballot_sync(GKM_FULL, j < mq && live && l - gkm_mism(u[j], v) >= a.min_matches);
+                unsigned hits = __ballot_sync(GKM_FULL, (hm >> j) & 1u);
                 while (hits) {
                     const int h = __ffs(hits) - 1;
                     hits &= hits - 1;
