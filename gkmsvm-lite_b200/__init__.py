@@ -6,7 +6,7 @@ kernels behind the C ABI of include/gkm_b200.h."""
 from .deltasvm import DeltaSVMWeights, deltasvm_weights
 from .explain import gkmexplain, mutation_impact
 from .gram import compute_gram
-from .importers import load_lsgkm_model, parse_lsgkm_header
+from .importers import load_classic_model, load_lsgkm_model, load_r_gkmsvm_model, parse_lsgkm_header, read_fasta
 from .inputs import as_batch, encode_codes, to_codes
 from .ism import ism
 from .kernels import (KERNEL_ALIASES, KERNEL_BUILDERS, CenterWeightedGkmKernel, CenterWeightedRbfGkmKernel,
@@ -23,5 +23,5 @@ __all__ = [
     "EstTruncGkmKernel", "CenterWeightedGkmKernel", "RbfKernel", "RbfGkmKernel",
     "CenterWeightedRbfGkmKernel", "as_batch", "encode_codes", "to_codes", "KernelColumnCache", "smo_solve",
     "smo_svr_solve", "DeltaSVMWeights", "deltasvm_weights", "parse_lsgkm_header", "load_npz", "save_npz",
-    "save_lsgkm", "load_deltasvm_npz", "save_deltasvm_npz",
+    "save_lsgkm", "load_deltasvm_npz", "save_deltasvm_npz", "load_classic_model", "load_r_gkmsvm_model", "read_fasta",
 ]

@@ -8,12 +8,13 @@ from __future__ import annotations
 
 import ctypes
 import gzip
+import re
 import warnings
 
 import numpy as np
 
 from . import _lib
-from .inputs import LSGKM_MAX_LENGTH
+from .inputs import LSGKM_MAX_LENGTH, as_batch, encode_codes
 from .kernels import KERNEL_ALIASES
 from .model import GkmSVM
 
@@ -118,3 +119,78 @@ def load_lsgkm_model(path, *, sv_chunk_size=None, device="cpu") -> GkmSVM:
     return GkmSVM(sv, coef, -header["rho"][0], header["kernel_type"], params,
                   sv_lengths=None if (lengths == longest).all() else lengths, sv_chunk_size=sv_chunk_size,
                   device=device)
+
+
+# gkmsvm_kernel -t (R useTgkm) filter types as kernel types, each cut at d
+# mismatches (importers/classic.py:23-26); 3 (wildcard) and 4 (mismatch
+# kernel) have no counterpart
+GKMSVM_FILTERS = {0: "gkm_estfull", 1: "gkm_esttrunc", 2: "gkm_cnt"}
+
+
+def read_fasta(path) -> list:
+    """(name, sequence) records of a FASTA file, gzip or plain (fasta.py:19-44)."""
+    records, name, seq = [], None, []
+    for line in _read_bytes(str(path)).decode("ascii", errors="replace").splitlines():
+        line = line.strip()
+        if not line:
+            continue
+        if line.startswith(">"):
+            if name is not None:
+                records.append((name, "".join(seq)))
+            name, seq = line[1:].strip(), []
+        else:
+            seq.append(line)
+    if name is not None:
+        records.append((name, "".join(seq)))
+    return records
+
+
+def load_classic_model(alpha_path, svseq_path=None, *, L: int = 10, k: int = 6, d: int = 3, filter_type: int = 1,
+                       include_rc: bool = True, sv_chunk_size=None, device="cpu") -> GkmSVM:
+    """GkmSVM of a model the classic gkmSVM tools (C++ or R) wrote
+    (importers/classic.py:29-120): PREFIX_svalpha.out ("id <TAB> alpha") and
+    PREFIX_svseq.fa, SVs matched to alphas by id with every letter other than
+    ACGT dropped, as the tools read them; the kernel comes from the arguments
+    (gkmsvm_kernel -l/-k/-d/-t, -R for no RC); bias 0."""
+    alpha_path = str(alpha_path)
+    if svseq_path is None:
+        if not alpha_path.endswith("svalpha.out"):
+            raise ValueError(f"give svseq_path for {alpha_path}")
+        svseq_path = alpha_path[: -len("svalpha.out")] + "svseq.fa"
+    ids, coefs = [], []
+    for line in _read_bytes(alpha_path).decode("ascii", errors="replace").splitlines():
+        parts = line.split()
+        if not parts:
+            continue
+        if len(parts) != 2:
+            raise ValueError(f"Expected 'id <TAB> alpha', got: {line.strip()[:80]}")
+        ids.append(parts[0])
+        coefs.append(float(parts[1]))
+    by_id = {name.split()[0]: seq for name, seq in read_fasta(svseq_path) if name.split()}
+    missing = [i for i in ids if i not in by_id]
+    if missing:
+        raise ValueError(f"{len(missing)} SV ids of {alpha_path} are not in {svseq_path}, e.g. {missing[0]}")
+    seqs = [re.sub("[^ACGTacgt]", "", by_id[i]).upper() for i in ids]
+    dropped = sum(len(by_id[i]) != len(s) for i, s in zip(ids, seqs))
+    if dropped:
+        warnings.warn(f"{dropped} support vectors hold letters other than ACGT, dropped as gkmSVM reads them "
+                      "(queries with N score as in gkmsvm_classify only with those letters dropped too)",
+                      stacklevel=2)
+    if filter_type not in GKMSVM_FILTERS:
+        raise NotImplementedError(f"gkmSVM filter type {filter_type} (wildcard/mismatch kernels) is not "
+                                  f"supported; use {sorted(GKMSVM_FILTERS)}")
+    if not seqs:
+        raise ValueError("No support vector sequences found")
+    codes = [encode_codes(s) for s in seqs]
+    sv, lengths = as_batch(codes)
+    params = {"L": L, "k": k, "d": d, "include_rc": bool(include_rc)}
+    return GkmSVM(sv, np.array(coefs, dtype=np.float64), 0.0, GKMSVM_FILTERS[filter_type], params,
+                  sv_lengths=lengths, sv_chunk_size=sv_chunk_size, device=device)
+
+
+def load_r_gkmsvm_model(path, svseq_path=None, *, L: int = 10, K: int = 6, maxnmm: int = 3, useTgkm: int = 1,
+                        addRC: bool = True, sv_chunk_size=None, device="cpu") -> GkmSVM:
+    """GkmSVM of a model R gkmSVM's gkmsvm_train wrote, the classic tools'
+    files, with the R package's argument names (importers/r_gkmsvm.py:17-53)."""
+    return load_classic_model(path, svseq_path, L=L, k=K, d=maxnmm, filter_type=useTgkm, include_rc=addRC,
+                              sv_chunk_size=sv_chunk_size, device=device)

@@ -9,7 +9,8 @@ self-kernels, scores, ISM, GkmExplain in three modes, variant scores, mutation
 impact, Gram), config1, config2, config3, config4, config5 (subsamples of the
 benchmark workloads), lsgkm (copies LS-GKM's gkmpredict / gkmexplain outputs
 and their models from gkmsvm-lite's test fixtures), deltasvm (to_deltasvm
-weights of the small models).  Inputs are regenerated in
+weights of the small models), gkmsvm (classic C++ / R gkmSVM models with the
+gkmSVM tools' own scores, from gkmsvm-lite's test fixtures).  Inputs are regenerated in
 the tests from the same seeds through gkmsvm_lite_b200.synthetic, or stored
 here when small.
 """
@@ -211,6 +212,22 @@ def lsgkm():
         f.write(f"random\t{rand_seq}\t-0.123703\n")
 
 
+GKMSVM_PREFIXES = ["gkmsvm_classic_t0", "gkmsvm_classic_t1", "gkmsvm_classic_t2", "gkmsvm_r_t1", "gkmsvm_r_t2"]
+
+
+def gkmsvm():
+    """Copies the classic C++ and R gkmSVM models of gkmsvm-lite's fixtures
+    (svalpha.out + svseq.fa, l=10 k=6 d=3) with gkmsvm_kernel's and
+    gkmsvm_classify's scores of the 100 and 85 bp test sets (the test FASTA
+    files are in lsgkm/)."""
+    dst = os.path.join(HERE, "gkmsvm")
+    os.makedirs(dst, exist_ok=True)
+    for p in GKMSVM_PREFIXES:
+        for suffix in ("_svalpha.out", "_svseq.fa", "_test100_kernel.txt", "_test85_kernel.txt",
+                       "_test100_classify.txt", "_test85_classify.txt"):
+            shutil.copy(os.path.join(REF_FIXTURES, p + suffix), os.path.join(dst, p + suffix))
+
+
 DELTASVM_FULL = 4**7  # weights stored whole up to this many, else a sample
 DELTASVM_SAMPLE = 8192
 
@@ -239,6 +256,7 @@ def deltasvm():
 
 
 if __name__ == "__main__":
-    groups = sys.argv[1:] or ["small", "config1", "config2", "config3", "config4", "config5", "lsgkm", "deltasvm"]
+    groups = sys.argv[1:] or ["small", "config1", "config2", "config3", "config4", "config5", "lsgkm", "deltasvm",
+                              "gkmsvm"]
     for g in groups:
         globals()[g]()
