@@ -451,6 +451,11 @@ def gram_leg(n=4000, forms=("index", "dense", "join")):
         out["raw_ms"][form] = {"ms": ms, "Gpairs_per_s": pairs / ms / 1e6, "identical_to_first": same}
         if form == "index":
             ix.close()
+    # the form the pairwise autotuner picks for this shape (its first call
+    # times both on a 64 x 4,096 sample)
+    engine.PAIRWISE_TUNED.clear()
+    engine.choose_pairwise(spec, bx, cx, bx, rx, cx)
+    out["pairwise_autotuned"] = {str(key): form for key, form in engine.PAIRWISE_TUNED.items()}
     return out
 
 

@@ -111,10 +111,17 @@ def dense_pairwise(spec: Spec, bx, cx, by, ry, cy, raw: bool = True, profile: bo
 
 
 # Pairwise method: "join" (warp ballot/popc over window pairs), "dense"
-# (tensor-core one-hot product), or "auto": the tensor-core product wherever
-# it applies (0 <= dmax < l <= 15).  Measured on B200 it runs 1.2x (60 bp
-# rows) to 4x (long rows, or dmax = 10) the join's window pairs per second.
+# (tensor-core one-hot product), or "auto": per shape class, the faster of the
+# forms that apply, measured on the first call of the class (the autotuner
+# below).  The two forms give identical results, so the choice changes only
+# the time.
 PAIRWISE_METHOD = "auto"
+
+# shape class -> "join" | "dense"; filled by the autotuner, read by bench/tests
+PAIRWISE_TUNED: dict = {}
+# rows and columns of the sample the autotuner times
+_TUNE_ROWS = 64
+_TUNE_COLS = 4096
 
 
 def hit_rate(l: int, dmax: int) -> float:
@@ -124,15 +131,67 @@ def hit_rate(l: int, dmax: int) -> float:
     return sum(comb(l, m) * 0.75 ** m * 0.25 ** (l - m) for m in range(dmax + 1))
 
 
-def choose_pairwise(spec: Spec, Wx: int) -> str:
-    return "dense" if dense_applies(spec) else "join"
+def pairwise_forms(spec: Spec) -> list:
+    """The pairwise forms that apply to the kernel: the join always, the
+    tensor-core product for 0 <= dmax < l <= 15."""
+    return ["join", "dense"] if dense_applies(spec) else ["join"]
+
+
+def _pow2(n: int) -> int:
+    return 1 << max(0, (int(n) - 1).bit_length())
+
+
+def pairwise_class(spec: Spec, B: int, Wx: int, S: int, Wy: int) -> tuple:
+    """The autotuner's shape class: the kernel's l, dmax, weighting and RC,
+    and the row/column counts and window widths rounded up to powers of two
+    (rows and columns capped where the per-pair cost has settled)."""
+    b = spec.base
+    return (b.l, b.dmax, bool(b.weighted), bool(b.include_rc), min(_pow2(B), 4096), _pow2(Wx),
+            min(_pow2(S), 65536), _pow2(Wy))
+
+
+def _time_form(form: str, spec: Spec, bx, cx, by, ry, cy) -> float:
+    fn = dense_pairwise if form == "dense" else join_pairwise
+    kw = {"check": False} if form == "dense" else {}
+    fn(spec, bx, cx, by, ry, cy)  # warm-up (and, for the dense form, its error check)
+    st = torch.cuda.current_stream()
+    best = float("inf")
+    for _ in range(2):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        fn(spec, bx, cx, by, ry, cy, **kw)
+        b.record(st)
+        b.synchronize()
+        best = min(best, a.elapsed_time(b))
+    return best
+
+
+def choose_pairwise(spec: Spec, bx, cx, by, ry, cy) -> str:
+    """The pairwise form for this call under "auto": the only one that
+    applies, or the one that ran a sample of the call (up to 64 rows x 4,096
+    columns) faster the first time its shape class was seen."""
+    forms = pairwise_forms(spec)
+    if len(forms) == 1:
+        return forms[0]
+    B, Wx = bx.shape
+    S, Wy = by.shape
+    key = pairwise_class(spec, B, Wx, S, Wy)
+    got = PAIRWISE_TUNED.get(key)
+    if got is None:
+        nb, ns = min(B, _TUNE_ROWS), min(S, _TUNE_COLS)
+        sample = (bx[:nb].contiguous(), cx[:nb].contiguous(), by[:ns].contiguous(),
+                  None if ry is None else ry[:ns].contiguous(), cy[:ns].contiguous())
+        times = {f: _time_form(f, spec, *sample) for f in forms}
+        got = min(forms, key=lambda f: times[f])
+        PAIRWISE_TUNED[key] = got
+    return got
 
 
 def pairwise(spec: Spec, bx, cx, by, ry, cy, raw: bool = True, profile: bool = False, method: str | None = None):
     """Pairwise K_raw / profiles through the join or the tensor-core kernel."""
     method = method or PAIRWISE_METHOD
     if method == "auto":
-        method = choose_pairwise(spec, int(bx.shape[1]))
+        method = choose_pairwise(spec, bx, cx, by, ry, cy)
     if method == "dense":
         return dense_pairwise(spec, bx, cx, by, ry, cy, raw, profile)
     if method != "join":

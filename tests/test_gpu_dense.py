@@ -99,3 +99,29 @@ def test_auto_pairwise_uses_dense_on_long_rows(monkeypatch):
     monkeypatch.setattr(engine, "PAIRWISE_METHOD", "dense")
     b = m(x, lengths=xl).cpu().numpy()
     np.testing.assert_array_equal(a, b)
+
+
+def test_autotuner_times_once_per_class_and_changes_no_result(monkeypatch):
+    """auto times both forms on the first call of a shape class, keeps the
+    faster, and reuses it; every form gives the same K_raw and profiles."""
+    monkeypatch.setattr(engine, "PAIRWISE_TUNED", {})
+    monkeypatch.setattr(engine, "PAIRWISE_METHOD", "auto")
+    rng = np.random.default_rng(11)
+    y, yl = _codes(rng, [300] * 40)
+    x, xl = _codes(rng, [280, 300, 120, 11])
+    m = gk.GkmSVM(y, np.linspace(-1, 1, 40), 0.0, "gkm_esttrunc", dict(L=11, k=7, d=3), sv_lengths=yl).cuda()
+    spec = m._spec()
+    by, ry, cy = m._sv_packed()
+    bx, _, cx = engine.pack(spec, torch.from_numpy(x).cuda(), xl)
+    raw, prof = engine.pairwise(spec, bx, cx, by, ry, cy, profile=True)
+    assert list(engine.PAIRWISE_TUNED.values()) in (["join"], ["dense"])
+    for form in ("join", "dense"):
+        r, p = engine.pairwise(spec, bx, cx, by, ry, cy, profile=True, method=form)
+        assert torch.equal(r, raw) and torch.equal(p, prof)
+
+    def timed_again(*a, **k):
+        raise AssertionError("the autotuner timed a class it had already measured")
+
+    monkeypatch.setattr(engine, "_time_form", timed_again)
+    r2, _ = engine.pairwise(spec, bx, cx, by, ry, cy)
+    assert torch.equal(r2, raw)

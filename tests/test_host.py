@@ -139,8 +139,9 @@ def test_abi_library_exports_every_declared_symbol():
     assert lib.gkm_version() >= 1
 
 
-def test_pairwise_dispatch_rule():
-    """auto takes the tensor-core product wherever it applies (dmax < l <= 15)."""
+def test_pairwise_forms_and_classes():
+    """The forms the autotuner chooses between (the tensor-core product only
+    where dmax < l <= 15), and its shape classes."""
     import torch
 
     from gkmsvm_lite_b200 import engine
@@ -153,6 +154,17 @@ def test_pairwise_dispatch_rule():
     # exact: l-mers within 3 of a given one, over all 4^11
     want = sum(comb(11, m) * 3 ** m for m in range(4)) / 4 ** 11
     assert abs(engine.hit_rate(11, 3) - want) < 1e-15
-    assert engine.choose_pairwise(spec("gkm_esttrunc", dict(L=11, k=7, d=3)), 50) == "dense"
-    assert engine.choose_pairwise(spec("gkm_cnt", dict(L=15, k=5, d=10)), 990) == "dense"
-    assert engine.choose_pairwise(spec("wgkm", dict(L=9, k=6, d=2)), 990) == "dense"
+    t2 = spec("gkm_esttrunc", dict(L=11, k=7, d=3))
+    assert engine.pairwise_forms(t2) == ["join", "dense"]
+    assert engine.pairwise_forms(spec("gkm_cnt", dict(L=15, k=5, d=10))) == ["join", "dense"]
+    assert engine.pairwise_forms(spec("wgkm", dict(L=9, k=6, d=2))) == ["join", "dense"]
+    # a kernel counting pairs at every mismatch level (dmax = l): the join only,
+    # chosen without timing
+    from types import SimpleNamespace
+    full = SimpleNamespace(base=SimpleNamespace(l=7, dmax=7))
+    assert engine.pairwise_forms(full) == ["join"]
+    assert engine.choose_pairwise(full, torch.zeros((3, 5), dtype=torch.int32), None,
+                                  torch.zeros((2, 8), dtype=torch.int32), None, None) == "join"
+    c = engine.pairwise_class(t2, 100, 290, 72000, 490)
+    assert c == (11, 3, False, True, 128, 512, 65536, 512)
+    assert engine.pairwise_class(t2, 65, 257, 5000, 300) == (11, 3, False, True, 128, 512, 8192, 512)
