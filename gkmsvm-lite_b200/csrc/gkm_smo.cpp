@@ -12,6 +12,16 @@
 // violation m(a) - M(a) is below tol.  The bias is -rho, rho the mean of
 // y_t G_t over free variables (or the midpoint of its bounds).
 //
+// Shrinking (the method of LIBSVM, Chang and Lin): every min(n, 1000)
+// iterations the variables at a bound whose gradient says they will stay
+// there leave the active set, and selection and gradient updates run over the
+// active set only.  G_bar_t = sum over variables at their upper bound of
+// C_s Q_ts is kept up to date (a column per bound change), so the gradient of
+// the inactive variables can be rebuilt from G_bar, p and the free variables'
+// columns: once when the violation first falls below 10 tol (then every
+// variable is active again and shrinking resumes), and when the active set
+// has converged, before the final check over all variables.
+//
 // Columns: an LRU cache of cache_columns columns of N doubles.  On a miss
 // the solver asks the provider for the column and, while the cache has free
 // slots, for up to prefetch - 1 more: the sequences of the variables most
@@ -104,15 +114,18 @@ struct Solver {
     int n, N;
     const double *y, *p, *diag;
     double Cp, Cn, tol;
-    std::vector<double> a, G;
+    std::vector<double> a, G, G_bar;
+    std::vector<int> active;  // the active variables, ascending
+    bool unshrunk = false;    // the one rebuild at 10 tol has happened
     ColumnCache cache;
     int prefetch;
 
     Solver(int n_, int N_, const double *y_, const double *p_, const double *diag_, double Cp_, double Cn_,
            double tol_, int cache_columns, int prefetch_, gkm_columns_cb cb, void *ctx)
         : n(n_), N(N_), y(y_), p(p_), diag(diag_), Cp(Cp_), Cn(Cn_), tol(tol_), a(n_, 0.0), G(p_, p_ + n_),
-          cache(N_, cache_columns, cb, ctx), prefetch(prefetch_)
+          G_bar(n_, 0.0), active(n_), cache(N_, cache_columns, cb, ctx), prefetch(prefetch_)
     {
+        for (int t = 0; t < n; t++) active[t] = t;
     }
 
     double C(int t) const { return y[t] > 0 ? Cp : Cn; }
@@ -129,7 +142,7 @@ struct Solver {
         const int k = std::min(prefetch - 1, cache.free_slots() - 1);
         if (k <= 0) return out;
         std::vector<std::pair<double, int>> up, low;
-        for (int t = 0; t < n; t++) {
+        for (int t : active) {
             const int c = t % N;
             if (c == skip || cache.cached(c)) continue;
             const double s = -y[t] * G[t];
@@ -160,7 +173,7 @@ struct Solver {
     {
         double Gmax = -INF, Gmax2 = -INF, best = INF;
         int i = -1, j = -1;
-        for (int t = 0; t < n; t++) {
+        for (int t : active) {
             if (!in_up(t)) continue;
             const double v = -y[t] * G[t];
             if (v >= Gmax) {
@@ -174,7 +187,7 @@ struct Solver {
             failed = true;
             return 0;
         }
-        for (int t = 0; t < n; t++) {
+        for (int t : active) {
             if (!in_low(t)) continue;
             const double v = -y[t] * G[t];
             if (-v >= Gmax2) Gmax2 = -v;
@@ -195,6 +208,73 @@ struct Solver {
         oi = i;
         oj = j;
         return 1;
+    }
+
+    // G_t for the inactive t from G_bar, p and the free variables' columns
+    // (inactive variables sit at a bound, so every free one is active);
+    // false if the provider failed
+    bool reconstruct()
+    {
+        if ((int)active.size() == n) return true;
+        std::vector<char> act(n, 0);
+        for (int t : active) act[t] = 1;
+        std::vector<int> idle;
+        for (int t = 0; t < n; t++)
+            if (!act[t]) {
+                idle.push_back(t);
+                G[t] = G_bar[t] + p[t];
+            }
+        for (int j : active) {
+            if (upper(j) || lower(j)) continue;
+            const double *Kj = column(j);
+            if (!Kj) return false;
+            const double c = y[j] * a[j];
+            for (int t : idle) G[t] += y[t] * c * Kj[t % N];
+        }
+        return true;
+    }
+
+    void activate_all()
+    {
+        active.resize(n);
+        for (int t = 0; t < n; t++) active[t] = t;
+    }
+
+    // drop the variables that will stay at their bound; false if the
+    // provider failed during the one rebuild
+    bool shrink()
+    {
+        double m = -INF, M = -INF;  // max over up of -y G, max over low of y G
+        for (int t : active) {
+            if (in_up(t)) m = std::max(m, -y[t] * G[t]);
+            if (in_low(t)) M = std::max(M, y[t] * G[t]);
+        }
+        if (!unshrunk && m + M <= 10.0 * tol) {
+            unshrunk = true;
+            if (!reconstruct()) return false;
+            activate_all();
+        }
+        std::vector<int> keep;
+        keep.reserve(active.size());
+        for (int t : active) {
+            bool drop = false;
+            if (upper(t))
+                drop = y[t] > 0 ? -G[t] > m : -G[t] > M;
+            else if (lower(t))
+                drop = y[t] > 0 ? G[t] > M : G[t] > m;
+            if (!drop) keep.push_back(t);
+        }
+        active.swap(keep);
+        return true;
+    }
+
+    // keep G_bar up to date for a variable whose upper-bound status changed;
+    // Kt its column
+    void bound_change(int t, bool was_upper, const double *Kt)
+    {
+        if (was_upper == upper(t)) return;
+        const double c = (was_upper ? -1.0 : 1.0) * C(t) * y[t];
+        for (int s = 0; s < n; s++) G_bar[s] += c * y[s] * Kt[s % N];
     }
 
     double rho() const
@@ -233,10 +313,28 @@ extern "C" int gkm_smo_solve(int32_t n, int32_t N, const double *y, const double
     Solver s(n, N, y, p, diag, C_pos, C_neg, tol, cache_columns, std::max(1, prefetch), columns, ctx);
     int64_t it = 0;
     bool failed = false;
+    int counter = std::min(n, 1000) + 1;
     for (; it < max_iter; it++) {
+        if (--counter == 0) {
+            counter = std::min(n, 1000);
+            if (!s.shrink()) {
+                failed = true;
+                break;
+            }
+        }
         int i = -1, j = -1;
         const double *Ki = nullptr;
-        if (!s.select(i, j, Ki, failed)) break;
+        if (!s.select(i, j, Ki, failed)) {
+            // converged on the active set: check every variable
+            if (failed || (int)s.active.size() == n) break;
+            if (!s.reconstruct()) {
+                failed = true;
+                break;
+            }
+            s.activate_all();
+            if (!s.select(i, j, Ki, failed)) break;
+            counter = 1;
+        }
         // Ki stays valid: fetching j evicts only the least recently used column
         // and i's was used last
         const double *Kj = s.column(j);
@@ -247,6 +345,7 @@ extern "C" int gkm_smo_solve(int32_t n, int32_t N, const double *y, const double
         Ki = s.column(i);  // i's column again (a hit; its storage did not move)
         const double Ci = s.C(i), Cj = s.C(j);
         const double ai0 = s.a[i], aj0 = s.a[j];
+        const bool ui = s.upper(i), uj = s.upper(j);
         double &ai = s.a[i], &aj = s.a[j];
         const double Kij = Ki[j % N];
         const double yi = y[i], yj = y[j];
@@ -304,10 +403,13 @@ extern "C" int gkm_smo_solve(int32_t n, int32_t N, const double *y, const double
         const double dai = ai - ai0, daj = aj - aj0;
         // G_t += Q_ti dai + Q_tj daj, Q_ts = y_t y_s K(t mod N, s mod N)
         const double ci = yi * dai, cj = yj * daj;
-        for (int t = 0; t < n; t++) s.G[t] += y[t] * (ci * Ki[t % N] + cj * Kj[t % N]);
+        for (int t : s.active) s.G[t] += y[t] * (ci * Ki[t % N] + cj * Kj[t % N]);
+        s.bound_change(i, ui, Ki);
+        s.bound_change(j, uj, Kj);
         if (verbose && (it + 1) % 100000 == 0)
             fprintf(stderr, "  SMO iteration %lld\n", (long long)(it + 1));
     }
+    if (!failed && !s.reconstruct()) failed = true;  // stopped by max_iter with variables shrunk
     if (failed) return gkm_fail(GKM_ERR_INVALID, "the kernel column provider failed");
     for (int t = 0; t < n; t++) coef[t] = y[t] * s.a[t];
     *bias = -s.rho();

@@ -87,3 +87,25 @@ def test_prefetch_batches_columns_and_provider_failure_stops():
     assert max(calls) > 1  # a miss fetched likely next columns with it
     with pytest.raises(ValueError, match="column provider"):
         _smo(K, y, -np.ones(50), (1.0, 1.0), cache=4, prefetch=1, fail_after=2)
+
+
+def test_shrinking_large_problems_equal_libsvm():
+    """1,500 sequences (C-SVC) and 700 (SVR, 1,400 dual variables): many
+    shrink rounds, the rebuild at 10 tol and the final full check."""
+    from sklearn.svm import SVC, SVR
+
+    K, rng = _kernel(1500, 3)
+    y = np.where(rng.random(1500) < 0.5, 1.0, -1.0)
+    y[rng.random(1500) < 0.1] *= -1  # label noise: bounded and free variables both
+    coef, bias, _ = _smo(K, y, -np.ones(1500), (1.0, 1.0), tol=1e-6, cache=400, prefetch=32)
+    ref = SVC(C=1.0, kernel="precomputed", tol=1e-6).fit(K, y)
+    np.testing.assert_allclose(K @ coef + bias, ref.decision_function(K), atol=2e-4)
+    want = np.zeros(1500)
+    want[ref.support_] = ref.dual_coef_[0]
+    assert np.abs(coef - want).max() < 1e-3
+    K2, rng = _kernel(700, 4)
+    z = np.sin(np.arange(700) / 30.0) + 0.1 * rng.normal(size=700)
+    signs = np.r_[np.ones(700), -np.ones(700)]
+    coef, bias, _ = _smo(K2, signs, np.r_[0.05 - z, 0.05 + z], (2.0, 2.0), tol=1e-6, cache=200, prefetch=16)
+    ref = SVR(C=2.0, epsilon=0.05, kernel="precomputed", tol=1e-6).fit(K2, z)
+    np.testing.assert_allclose(K2 @ (coef[:700] + coef[700:]) + bias, ref.predict(K2), atol=2e-4)
