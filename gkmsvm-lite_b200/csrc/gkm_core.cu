@@ -15,6 +15,11 @@ namespace {
 constexpr int SELF_THREADS = 256;
 constexpr int SMEM_WINDOWS = 12288;  // rows staged in shared memory up to this
 
+// staged-window capacity of a launch over rows of W window slots: the
+// shared memory is sized to the rows, not to the limit, so short rows leave
+// room for more blocks per SM
+static int staged_windows(int64_t W) { return (int)(W < 1 ? 1 : W < SMEM_WINDOWS ? W : SMEM_WINDOWS); }
+
 // ---------------------------------------------------------------------------
 // Packing (kernels/packed.py:130-187)
 // ---------------------------------------------------------------------------
@@ -137,18 +142,19 @@ __device__ void block_reduce_levels(uint64_t *tot, uint64_t *red, uint64_t *sums
     __syncthreads();
 }
 
+// sw: windows the shared memory holds per strand (2 * sw words)
 __device__ __forceinline__ RowView stage_row(const uint32_t *fwd, const uint32_t *rc, int64_t W,
-                                             int n, bool has_rc, uint32_t *sm)
+                                             int n, bool has_rc, uint32_t *sm, int sw)
 {
     RowView rv;
     rv.W = W;
-    if (n <= SMEM_WINDOWS) {
+    if (n <= sw) {
         for (int k = threadIdx.x; k < n; k += blockDim.x) {
             sm[k] = fwd[k];
-            if (has_rc) sm[SMEM_WINDOWS + k] = rc[W - 1 - k];
+            if (has_rc) sm[sw + k] = rc[W - 1 - k];
         }
         rv.f = sm;
-        rv.r = sm + SMEM_WINDOWS;
+        rv.r = sm + sw;
         rv.reversed = false;
     } else {
         rv.f = fwd;
@@ -166,7 +172,7 @@ __global__ void __launch_bounds__(SELF_THREADS) self_kernel(
     gkm_spec spec, const uint32_t *__restrict__ fwd, const uint32_t *__restrict__ rc,
     const int32_t *__restrict__ counts, int64_t W, double *__restrict__ diag,
     uint64_t *__restrict__ profile, const double *__restrict__ table, double bias, int normalize,
-    double *__restrict__ scores, double *__restrict__ raw_out)
+    double *__restrict__ scores, double *__restrict__ raw_out, int sw)
 {
     constexpr int NL = 4 * NW;
     extern __shared__ uint32_t sm[];
@@ -177,7 +183,7 @@ __global__ void __launch_bounds__(SELF_THREADS) self_kernel(
     int n = counts[b];
     bool has_rc = spec.include_rc && rc != nullptr;
     const uint32_t *frow = fwd + b * W;
-    RowView rv = stage_row(frow, has_rc ? rc + b * W : nullptr, W, n, has_rc, sm);
+    RowView rv = stage_row(frow, has_rc ? rc + b * W : nullptr, W, n, has_rc, sm, sw);
     uint64_t tot[NL];
 #pragma unroll
     for (int m = 0; m < NL; m++) tot[m] = 0;
@@ -328,7 +334,7 @@ __global__ void __launch_bounds__(MUT_THREADS) mutant_kernel(
     gkm_spec spec, const uint32_t *__restrict__ fwd, const int32_t *__restrict__ counts, int64_t B,
     int64_t W, int64_t L, const double *__restrict__ diag, double *__restrict__ mut_diag,
     const double *__restrict__ table, const double *__restrict__ ref_raw, int normalize,
-    double *__restrict__ ism_out)
+    double *__restrict__ ism_out, int sw)
 {
     constexpr int NL = 4 * NW;
     constexpr int NA = 5;  // old, new v = 0..3
@@ -351,12 +357,12 @@ __global__ void __launch_bounds__(MUT_THREADS) mutant_kernel(
     bool has_rc = spec.include_rc != 0;
     const uint32_t *frow = fwd + b * W;
     uint32_t *f = sm;  // [n] forward, [n] rc(f)
-    bool in_smem = n <= SMEM_WINDOWS;
+    bool in_smem = n <= sw;
     if (in_smem) {
         for (int k = threadIdx.x; k < n; k += blockDim.x) {
             uint32_t w = frow[k];
             f[k] = w;
-            f[SMEM_WINDOWS + k] = gkm_rc_word(w, l);
+            f[sw + k] = gkm_rc_word(w, l);
         }
         __syncthreads();
     }
@@ -372,7 +378,7 @@ __global__ void __launch_bounds__(MUT_THREADS) mutant_kernel(
     if (diag || mut_diag) {
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
             uint32_t fj = F[j];
-            uint32_t rj = in_smem ? f[SMEM_WINDOWS + j] : gkm_rc_word(fj, l);
+            uint32_t rj = in_smem ? f[sw + j] : gkm_rc_word(fj, l);
             bool jin = j >= a_s && j < a_e;
             uint64_t wj = wt ? gkm_wt(wd, n, j) : 1;
             Packed<NW> acc[NA];
@@ -560,14 +566,15 @@ static int self_launch(const gkm_spec *spec, const uint32_t *fwd, const uint32_t
                        int normalize, double *scores, double *raw, cudaStream_t st)
 {
     if (B == 0) return GKM_OK;
-    size_t smem = (size_t)2 * SMEM_WINDOWS * sizeof(uint32_t);
+    const int sw = staged_windows(W);
+    size_t smem = (size_t)2 * sw * sizeof(uint32_t);
     int nw = nw_for(spec->dmax);
 #define GKM_SELF(NW)                                                                                  \
     do {                                                                                              \
         cudaFuncSetAttribute(self_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
         self_kernel<NW><<<(unsigned)B, SELF_THREADS, smem, st>>>(*spec, fwd, rc, counts, W, diag,      \
                                                                  profile, table, bias, normalize,     \
-                                                                 scores, raw);                        \
+                                                                 scores, raw, sw);                    \
     } while (0)
     if (nw == 1) GKM_SELF(1);
     else if (nw == 2) GKM_SELF(2);
@@ -679,14 +686,15 @@ static int mutant_launch(const gkm_spec *spec, const uint32_t *fwd, const int32_
 {
     if (B == 0 || L == 0) return GKM_OK;
     if (B > 65535) return gkm_fail(GKM_ERR_UNSUPPORTED, "more than 65,535 rows per ISM launch");
-    size_t smem = (size_t)2 * SMEM_WINDOWS * sizeof(uint32_t);
+    const int sw = staged_windows(W);
+    size_t smem = (size_t)2 * sw * sizeof(uint32_t);
     dim3 grid((unsigned)L, (unsigned)B);
     int nw = nw_for(spec->dmax);
 #define GKM_MUT(NW)                                                                                      \
     do {                                                                                                 \
         cudaFuncSetAttribute(mutant_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
         mutant_kernel<NW><<<grid, MUT_THREADS, smem, st>>>(*spec, fwd, counts, B, W, L, diag, mut_diag,  \
-                                                           table, ref_raw, normalize, out);              \
+                                                           table, ref_raw, normalize, out, sw);          \
     } while (0)
     if (nw == 1) GKM_MUT(1);
     else if (nw == 2) GKM_MUT(2);
