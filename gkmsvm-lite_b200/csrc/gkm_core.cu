@@ -337,7 +337,9 @@ __global__ void __launch_bounds__(MUT_THREADS) mutant_kernel(
     double *__restrict__ ism_out, int sw)
 {
     constexpr int NL = 4 * NW;
-    constexpr int NA = 5;  // old, new v = 0..3
+    // the pair counts with base v at p, v = 0..3; the reference base's are
+    // the row's own (its substitution changes nothing), so they serve as "old"
+    constexpr int NA = 4;
     extern __shared__ uint32_t sm[];
     __shared__ uint64_t red[(MUT_THREADS / 32) * NA * NL];
     __shared__ uint64_t sums[NA * NL];
@@ -368,6 +370,7 @@ __global__ void __launch_bounds__(MUT_THREADS) mutant_kernel(
     }
     const uint32_t *F = in_smem ? f : frow;
     const int na = a_e - a_s;
+    const int xp = (int)((F[a_s] >> (2 * (p - a_s))) & 3u);  // the row's base at p
     const uint8_t *wd = spec.wd;
     const bool wt = spec.weighted != 0;
     uint64_t tot[NA][NL];
@@ -390,8 +393,6 @@ __global__ void __launch_bounds__(MUT_THREADS) mutant_kernel(
                 uint64_t wi = wt ? gkm_wt(wd, n, i) : 1;
                 uint32_t sh = 2u * (uint32_t)(p - i);
                 uint32_t cleared = fi & ~(3u << sh);
-                acc[0].add((uint32_t)gkm_mism(fi, fj), wi);
-                if (has_rc) acc[0].add((uint32_t)gkm_mism(fi, rj), wi);
 #pragma unroll
                 for (int v = 0; v < 4; v++) {
                     uint32_t fn = cleared | ((uint32_t)v << sh);
@@ -401,8 +402,8 @@ __global__ void __launch_bounds__(MUT_THREADS) mutant_kernel(
                         gj = (fj & ~(3u << shj)) | ((uint32_t)v << shj);
                         grj = gkm_rc_word(gj, l);
                     }
-                    acc[1 + v].add((uint32_t)gkm_mism(fn, gj), wi);
-                    if (has_rc) acc[1 + v].add((uint32_t)gkm_mism(fn, grj), wi);
+                    acc[v].add((uint32_t)gkm_mism(fn, gj), wi);
+                    if (has_rc) acc[v].add((uint32_t)gkm_mism(fn, grj), wi);
                 }
             }
             uint64_t scale = (jin ? 1 : 2) * wj;  // 2 * 11 * 255 < 2^16
@@ -434,7 +435,7 @@ __global__ void __launch_bounds__(MUT_THREADS) mutant_kernel(
         if (diag || mut_diag) {
             double delta = 0.0;
             for (int m = 0; m < NL && m <= spec.dmax; m++) {
-                int64_t dn = (int64_t)(sums[(1 + v) * NL + m] - sums[m]);
+                int64_t dn = (int64_t)(sums[v * NL + m] - sums[xp * NL + m]);
                 delta += spec.h[m] * (double)dn;
             }
             md = d0 + delta;
