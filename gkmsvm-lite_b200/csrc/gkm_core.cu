@@ -392,16 +392,31 @@ __global__ void __launch_bounds__(MUT_THREADS) mutant_kernel(
                 uint32_t fi = F[i];
                 uint64_t wi = wt ? gkm_wt(wd, n, i) : 1;
                 uint32_t sh = 2u * (uint32_t)(p - i);
+                if (!jin) {
+                    // only window i changes: its mismatches with j away from
+                    // offset k = p - i, plus one where j's base at k is not v
+                    const uint32_t keep = ~(1u << sh);
+                    uint32_t x = fi ^ fj;
+                    const uint32_t mf = (uint32_t)__popc((x | (x >> 1)) & 0x55555555u & keep);
+                    const uint32_t bf = (fj >> sh) & 3u;
+                    x = fi ^ rj;
+                    const uint32_t mr = (uint32_t)__popc((x | (x >> 1)) & 0x55555555u & keep);
+                    const uint32_t br = (rj >> sh) & 3u;
+#pragma unroll
+                    for (int v = 0; v < 4; v++) {
+                        acc[v].add(mf + (bf != (uint32_t)v), wi);
+                        if (has_rc) acc[v].add(mr + (br != (uint32_t)v), wi);
+                    }
+                    continue;
+                }
                 uint32_t cleared = fi & ~(3u << sh);
 #pragma unroll
                 for (int v = 0; v < 4; v++) {
                     uint32_t fn = cleared | ((uint32_t)v << sh);
-                    uint32_t gj = fj, grj = rj;
-                    if (jin) {  // both windows change
-                        uint32_t shj = 2u * (uint32_t)(p - j);
-                        gj = (fj & ~(3u << shj)) | ((uint32_t)v << shj);
-                        grj = gkm_rc_word(gj, l);
-                    }
+                    // both windows change
+                    const uint32_t shj = 2u * (uint32_t)(p - j);
+                    const uint32_t gj = (fj & ~(3u << shj)) | ((uint32_t)v << shj);
+                    const uint32_t grj = gkm_rc_word(gj, l);
                     acc[v].add((uint32_t)gkm_mism(fn, gj), wi);
                     if (has_rc) acc[v].add((uint32_t)gkm_mism(fn, grj), wi);
                 }
