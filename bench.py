@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--queries", type=int, default=100000)
     ap.add_argument("--no-extras", action="store_true", help="skip t=2, plain-call and CPU legs")
-    ap.add_argument("--leg", default="all", choices=["all", "gram", "train", "explain", "explain-pairs"],
+    ap.add_argument("--leg", default="all", choices=["all", "gram", "train", "explain", "explain-pairs", "serve"],
                     help="gram / train / explain: run only the Gram-matrix, SMO training or config-4 ISM and "
                          "GkmExplain leg (one GPU), print its JSON")
     ap.add_argument("--gram-n", type=int, default=4000, help="sequences of the Gram-matrix leg")
@@ -690,6 +690,11 @@ def main():
         return 0
     if args.leg == "train":
         print(json.dumps(training_leg(args.gram_n)), flush=True)
+        return 0
+    if args.leg == "serve":
+        import gkmsvm_lite_b200.synthetic as syn
+
+        print(json.dumps(serving_leg(*syn.config3_model())), flush=True)
         return 0
     if args.leg == "explain-pairs":
         print(json.dumps(explain_pairs_leg()), flush=True)

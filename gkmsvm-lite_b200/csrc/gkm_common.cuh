@@ -126,5 +126,12 @@ struct gkm_index {
 // work-queue counter; more than this many in flight at once would share one.
 #define GKM_QUEUE_SLOTS 64
 
+// Kernels that run beside the index query (other streams of a serving loop)
+// ask for the largest shared-memory carveout, the one the query needs: an SM
+// whose blocks use another carveout must drain before the query's block can
+// start on it.
+#define GKM_PREFER_SHARED(fn) cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, \
+                                                   (int)cudaSharedmemCarveoutMaxShared)
+
 int gkm_smem_limit();
 int gkm_sm_count();

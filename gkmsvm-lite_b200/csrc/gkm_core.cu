@@ -572,6 +572,7 @@ extern "C" int gkm_pack(const gkm_spec *spec, const uint8_t *codes, const int64_
     int64_t W = L - spec->l + 1;
     int64_t n = B * W;
     if (n == 0) return GKM_OK;
+    GKM_PREFER_SHARED(pack_kernel);
     pack_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(codes, lengths, B, L, spec->l, fwd, rc, counts);
     GKM_CHECK_LAUNCH("pack");
     return GKM_OK;
@@ -588,6 +589,7 @@ static int self_launch(const gkm_spec *spec, const uint32_t *fwd, const uint32_t
 #define GKM_SELF(NW)                                                                                  \
     do {                                                                                              \
         cudaFuncSetAttribute(self_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        GKM_PREFER_SHARED(self_kernel<NW>);                                                            \
         self_kernel<NW><<<(unsigned)B, SELF_THREADS, smem, st>>>(*spec, fwd, rc, counts, W, diag,      \
                                                                  profile, table, bias, normalize,     \
                                                                  scores, raw, sw);                    \
@@ -709,6 +711,7 @@ static int mutant_launch(const gkm_spec *spec, const uint32_t *fwd, const int32_
 #define GKM_MUT(NW)                                                                                      \
     do {                                                                                                 \
         cudaFuncSetAttribute(mutant_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+        GKM_PREFER_SHARED(mutant_kernel<NW>);                                                            \
         mutant_kernel<NW><<<grid, MUT_THREADS, smem, st>>>(*spec, fwd, counts, B, W, L, diag, mut_diag,  \
                                                            table, ref_raw, normalize, out, sw);          \
     } while (0)
@@ -746,6 +749,7 @@ extern "C" int gkm_raw_score(const double *raw, int64_t B, int64_t S, const doub
                              gkm_stream_t stream)
 {
     if (B == 0) return GKM_OK;
+    GKM_PREFER_SHARED(raw_score_kernel);
     raw_score_kernel<<<(unsigned)B, 256, 0, (cudaStream_t)stream>>>(raw, S, dx, ds, coef, gamma, rbf, bias, scores);
     GKM_CHECK_LAUNCH("raw_score");
     return GKM_OK;
@@ -755,6 +759,7 @@ extern "C" int gkm_impact(const double *raw, int64_t n, int64_t S, const double 
                           const double *coef, double gamma, int32_t rbf, double *out, gkm_stream_t stream)
 {
     if (n == 0) return GKM_OK;
+    GKM_PREFER_SHARED(impact_kernel);
     impact_kernel<<<(unsigned)n, 256, 0, (cudaStream_t)stream>>>(raw, n, S, dr, ds, coef, gamma, rbf, out);
     GKM_CHECK_LAUNCH("impact");
     return GKM_OK;

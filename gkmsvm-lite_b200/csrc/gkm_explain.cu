@@ -315,12 +315,14 @@ extern "C" int gkm_explain_lmer(const gkm_spec *spec, const uint32_t *fwd, const
     a.perturbation = perturbation;
     a.part = part;
     dim3 grid((unsigned)((W + EX_WARPS - 1) / EX_WARPS), (unsigned)B);
+    GKM_PREFER_SHARED(explain_windows);
     explain_windows<<<grid, EX_WARPS * 32, 0, st>>>(a);
     int s = GKM_OK;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) s = gkm_cuda_status(e, "explain_windows");
     if (s == GKM_OK) {
         int64_t n = B * 4 * L;
+        GKM_PREFER_SHARED(explain_gather);
         explain_gather<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, counts, B, W, L, spec->l, inv_dx, out);
         e = cudaGetLastError();
         if (e != cudaSuccess) s = gkm_cuda_status(e, "explain_gather");
@@ -381,6 +383,7 @@ extern "C" int gkm_explain_pairs(const gkm_spec *spec, const uint32_t *fwd, cons
     }
     if (s == GKM_OK) {
         int64_t n = B * 4 * L;
+        GKM_PREFER_SHARED(explain_gather);
         explain_gather<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, counts, B, W, L, spec->l, inv_dx, out,
                                                                     nsplit);
         cudaError_t e = cudaGetLastError();

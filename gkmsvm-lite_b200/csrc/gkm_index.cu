@@ -913,6 +913,7 @@ extern "C" int gkm_index_pairwise(const gkm_index_t *ix, const uint32_t *bx, con
         CountFinish f = count_finish_args(ix, g, B);
         f.raw = raw;
         f.profile = profile;
+        GKM_PREFER_SHARED(count_finish_raw);
         count_finish_raw<<<(unsigned)((B * ix->S + 255) / 256), 256, 0, st>>>(f);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) s = gkm_cuda_status(e, "count_finish_raw");
@@ -956,6 +957,7 @@ extern "C" int gkm_index_score(const gkm_index_t *ix, const uint32_t *bx, const 
             f.gamma = gamma;
             f.rbf = rbf;
             f.partial = partial;
+            GKM_PREFER_SHARED(count_finish_score);
             count_finish_score<<<dim3((unsigned)ix->tiles, (unsigned)B), 256, 0, st>>>(f);
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) s = gkm_cuda_status(e, "count_finish_score");
@@ -963,7 +965,9 @@ extern "C" int gkm_index_score(const gkm_index_t *ix, const uint32_t *bx, const 
         if (g) cudaFreeAsync(g, st);
     }
     if (s == GKM_OK) {
-        finish_scores<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(partial, B, ix->tiles, bias, scores);
+        GKM_PREFER_SHARED(finish_scores);
+        GKM_PREFER_SHARED(finish_scores);
+    finish_scores<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(partial, B, ix->tiles, bias, scores);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) s = gkm_cuda_status(e, "finish_scores");
     }
@@ -1141,6 +1145,7 @@ extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, con
         int64_t np = chunk / B;
         if (p0 + np > L) np = L - p0;
         int64_t nitems = np * B;
+        GKM_PREFER_SHARED(ism_sets_kernel);
         ism_sets_kernel<<<(unsigned)((nitems + 127) / 128), 128, 0, st>>>(ix->spec, fwd, counts, B, W, p0, nitems,
                                                                            rows, rc, rw);
         cudaError_t e = cudaGetLastError();
@@ -1152,6 +1157,7 @@ extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, con
         a.wq = ix->spec.weighted ? rw : nullptr;
         a.raw = kset;
         if ((s = query_launch<MODE_RAW>(ix, a, nitems * ISM_SETS, st)) != GKM_OK) break;
+        GKM_PREFER_SHARED(ism_index_finish);
         ism_index_finish<<<(unsigned)nitems, 256, 0, st>>>(kset, S, fwd, counts, B, W, L, l, p0, ref_raw, ref_score,
                                                            inv_dx, inv_dmut, inv_ds, coef, gamma, rbf, out);
         e = cudaGetLastError();
