@@ -292,8 +292,14 @@ class GpuBackend:
         self._busy = [False] * slots
 
     def free_memory(self) -> int:
-        free, _ = self.torch.cuda.mem_get_info()
-        return int(free)
+        """Bytes a new request can use: the device's free memory plus what
+        torch's caching allocator holds but no tensor uses (it reuses that
+        before asking the device; mem_get_info alone would count it as taken
+        for as long as the cache keeps it)."""
+        torch = self.torch
+        free, _ = torch.cuda.mem_get_info()
+        cached = torch.cuda.memory_reserved() - torch.cuda.memory_allocated()
+        return int(free + max(cached, 0))
 
     def prepare(self, r: Request):
         from .inputs import allele_arrays, as_batch
