@@ -168,3 +168,32 @@ def test_pairwise_forms_and_classes():
     c = engine.pairwise_class(t2, 100, 290, 72000, 490)
     assert c == (11, 3, False, True, 128, 512, 65536, 512)
     assert engine.pairwise_class(t2, 65, 257, 5000, 300) == (11, 3, False, True, 128, 512, 8192, 512)
+
+
+def test_pairwise_autotuner_caches_per_class(monkeypatch):
+    """The autotuner times each form once per shape class (here with a fake
+    clock: the join is faster on short rows, the tensor-core form on long
+    ones) and reuses the choice."""
+    import torch
+
+    from gkmsvm_lite_b200 import engine
+
+    m = gk.GkmSVM(np.zeros((2, 40), np.uint8), np.ones(2), 0.0, "gkm_esttrunc", dict(L=11, k=7, d=3))
+    spec = engine.Spec(m.kernel.base, torch.device("cpu"))
+    timed = []
+
+    def fake_time(form, spec_, bx, cx, by, ry, cy):
+        timed.append((form, bx.shape[1]))
+        return (1.0 if form == "join" else 2.0) if bx.shape[1] < 100 else (3.0 if form == "join" else 1.0)
+
+    monkeypatch.setattr(engine, "_time_form", fake_time)
+    monkeypatch.setattr(engine, "PAIRWISE_TUNED", {})
+    i32 = lambda *s: torch.zeros(s, dtype=torch.int32)
+    short, long_ = i32(10, 50), i32(10, 900)
+    cols, ccount = i32(300, 290), i32(300)
+    assert engine.choose_pairwise(spec, short, i32(10), cols, cols, ccount) == "join"
+    assert engine.choose_pairwise(spec, short, i32(10), cols, cols, ccount) == "join"
+    assert engine.choose_pairwise(spec, long_, i32(10), cols, cols, ccount) == "dense"
+    assert engine.choose_pairwise(spec, i32(12, 1000), i32(12), cols, cols, ccount) == "dense"  # same class
+    assert sorted(timed) == [("dense", 50), ("dense", 900), ("join", 50), ("join", 900)]
+    assert len(engine.PAIRWISE_TUNED) == 2
