@@ -10,7 +10,8 @@ impact, Gram), config1, config2, config3, config4, config5 (subsamples of the
 benchmark workloads), lsgkm (copies LS-GKM's gkmpredict / gkmexplain outputs
 and their models from gkmsvm-lite's test fixtures), deltasvm (to_deltasvm
 weights of the small models), gkmsvm (classic C++ / R gkmSVM models with the
-gkmSVM tools' own scores, from gkmsvm-lite's test fixtures).  Inputs are regenerated in
+gkmSVM tools' own scores, from gkmsvm-lite's test fixtures), files (model
+files gkmsvm-lite's serialization writes).  Inputs are regenerated in
 the tests from the same seeds through gkmsvm_lite_b200.synthetic, or stored
 here when small.
 """
@@ -228,6 +229,29 @@ def gkmsvm():
             shutil.copy(os.path.join(REF_FIXTURES, p + suffix), os.path.join(dst, p + suffix))
 
 
+def files():
+    """Model files written by gkmsvm-lite itself (serialization.py): the t4
+    and t2norc small models as npz and LS-GKM text (plain and gzip), and the
+    t0small model's DeltaSVM weights as npz."""
+    from gkmsvm.serialization import save_deltasvm_npz, save_lsgkm, save_npz
+
+    dst = os.path.join(HERE, "files")
+    os.makedirs(dst, exist_ok=True)
+    for name, kt, params, n_sv, svr, n_q, qr, seed in SMALL:
+        if name not in ("t4", "t2norc", "t0small"):
+            continue
+        rng = np.random.default_rng(seed)
+        sv, svl = _ragged(rng, n_sv, *svr)
+        coef = rng.normal(size=n_sv)
+        m = GkmSVM(sv, coef, -0.15, kt, params, sv_lengths=svl)
+        if name == "t0small":
+            save_deltasvm_npz(m.to_deltasvm(), os.path.join(dst, f"{name}_deltasvm.npz"))
+            continue
+        save_npz(m, os.path.join(dst, f"{name}.npz"))
+        save_lsgkm(m, os.path.join(dst, f"{name}.model.txt"))
+        save_lsgkm(m, os.path.join(dst, f"{name}.model.txt.gz"))
+
+
 DELTASVM_FULL = 4**7  # weights stored whole up to this many, else a sample
 DELTASVM_SAMPLE = 8192
 
@@ -257,6 +281,6 @@ def deltasvm():
 
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "config1", "config2", "config3", "config4", "config5", "lsgkm", "deltasvm",
-                              "gkmsvm"]
+                              "gkmsvm", "files"]
     for g in groups:
         globals()[g]()

@@ -194,3 +194,33 @@ def test_parser_counts_then_fills():
     assert other == 1
     coef, codes, lengths, other = importers.parse_lsgkm_svs(b"")
     assert coef.shape == (0,) and codes.shape == (0, 0)
+
+
+FILES = os.path.join(os.path.dirname(LSGKM), "files")
+
+
+@pytest.mark.parametrize("name", ["t4", "t2norc"])
+@pytest.mark.parametrize("ext", [".npz", ".model.txt", ".model.txt.gz"])
+def test_reads_files_gkmsvm_lite_wrote(small, name, ext):
+    """npz and LS-GKM text written by gkmsvm-lite's own serialization load to
+    the model they were written from."""
+    c = small[name]
+    m = gk.load_model(os.path.join(FILES, name + ext))
+    assert m.kernel_type == c["kernel_type"]
+    assert m.bias == pytest.approx(float(c["bias"]), abs=0 if ext == ".npz" else 1e-15)
+    for key, value in c["params"].items():
+        assert m.kernel_params.get(key, value) == value
+    assert m.kernel.include_rc == c["params"].get("include_rc", True)
+    np.testing.assert_array_equal(m.coefficients, c["coef"])
+    lengths = np.asarray(c["sv_lengths"])
+    np.testing.assert_array_equal(np.asarray(m.sv_lengths), lengths)
+    for i, n in enumerate(lengths):
+        np.testing.assert_array_equal(m.support_sequences[i, :n], c["sv"][i, :n])
+
+
+def test_reads_deltasvm_npz_gkmsvm_lite_wrote():
+    d = gk.load_model(os.path.join(FILES, "t0small_deltasvm.npz"))
+    assert (d.l, d.k, d.include_rc) == (3, 3, False) and d.bias == -0.15
+    assert d.weights.shape == (64,)
+    z = np.load(os.path.join(os.path.dirname(LSGKM), "deltasvm.npz"))
+    np.testing.assert_array_equal(d.weights, z["t0small/w"])
