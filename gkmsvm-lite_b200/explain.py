@@ -22,8 +22,7 @@ import torch
 
 from . import engine
 from ._lib import call, ptr, stream_handle
-from .inputs import (allele_arrays, as_batch, device_codes, joint_lengths, nan_rows, per_position, rows,
-                     short_rows)
+from .inputs import SeqBatch, allele_batches, device_codes, nan_rows, per_position
 from .kernels import INDEX_MAX_L, MAX_NEIGHBORS, RbfKernel, explain_tables, neighbor_count, neighbor_masks
 
 _MODE_ALIASES = {0: "importance", 1: "hypothetical", 2: "perturbation", "importance": "importance",
@@ -142,13 +141,12 @@ def gkmexplain(model, x, *, mode="importance", lengths=None, batch_size=50, verb
     if resolved is None:
         raise ValueError(f"mode must be 'importance', 'hypothetical', or 'perturbation' (or 0/1/2), got {mode!r}")
     dev = model._require_gpu()
-    x, lengths = as_batch(x, lengths)
-    short = short_rows(lengths, model.kernel.base.l, "attributions")
-    B, L = x.shape
+    batch = SeqBatch.read(x, lengths)
+    short = batch.short(model.kernel.base.l, "attributions")
+    B = batch.B
     bs = max(1, int(batch_size)) if batch_size else B
     # the table (if any) is chosen for the whole call, as the reference does
-    n_windows = int(np.clip(np.asarray(lengths if lengths is not None else np.full(B, L)) - model.kernel.base.l + 1,
-                            0, None).sum())
+    n_windows = batch.n_windows(model.kernel.base.l)
     table = _explain_table(model, n_windows, resolved == "perturbation", dev)
     parts = []
     it = range(0, B, bs)
@@ -156,9 +154,10 @@ def gkmexplain(model, x, *, mode="importance", lengths=None, batch_size=50, verb
         from tqdm import tqdm
         it = tqdm(it, desc="GkmExplain")
     for s in it:
-        parts.append(_explain_rows(model, x[s:s + bs], rows(lengths, s, bs), resolved, dev, table))
+        p = batch.part(s, bs)
+        parts.append(_explain_rows(model, p.codes, p.lengths, resolved, dev, table))
     out = parts[0] if len(parts) == 1 else torch.cat(parts)
-    return per_position(out, lengths, short)
+    return per_position(out, batch, short)
 
 
 def _explain_rows(model, x, lengths, mode, dev, table=None):
@@ -236,15 +235,11 @@ def mutation_impact(model, ref, alt, *, ref_lengths=None, alt_lengths=None, batc
     dev = model._require_gpu()
     kernel = model.kernel
     base = kernel.base
-    ref, alt, ref_lengths, alt_lengths = allele_arrays(ref, alt, ref_lengths, alt_lengths)
-    L = ref.shape[-1]
-    B = ref.shape[0]
-    short = None
-    if ref_lengths is not None or alt_lengths is not None:
-        both_l = joint_lengths(L, (B, ref_lengths), (B, alt_lengths))
-        s = short_rows(both_l, base.l, "mutation impacts")
-        if s is not None:
-            short = s.reshape(2, -1).any(axis=0)
+    rb, ab = allele_batches(ref, alt, ref_lengths, alt_lengths)
+    L, B = rb.L, rb.B
+    # a variant whose reference or alternative allele has no window is NaN
+    s = SeqBatch.stacked(rb, ab).short(base.l, "mutation impacts")
+    short = None if s is None else s.reshape(2, -1).any(axis=0)
     W = max(L - base.l + 1, 0)
     model._plan_lmer_table(B * 2 * (min(base.l, W) if model._index_applies() else W))
     if L < base.l:
@@ -255,11 +250,9 @@ def mutation_impact(model, ref, alt, *, ref_lengths=None, alt_lengths=None, batc
     rbf = isinstance(kernel, RbfKernel)
     gamma = kernel.gamma if rbf else 0.0
     for s in range(0, B, bs):
-        r, a = ref[s:s + bs], alt[s:s + bs]
-        n = r.shape[0]
-        both = torch.cat([device_codes(r, dev), device_codes(a, dev)])
-        bl = joint_lengths(L, (n, rows(ref_lengths, s, bs)), (n, rows(alt_lengths, s, bs)))
-        fwd, rc, counts = engine.pack(spec, both, bl)
+        pair = SeqBatch.stacked(rb.part(s, bs), ab.part(s, bs))
+        n = pair.B // 2
+        fwd, rc, counts = engine.pack(spec, pair.on(dev), pair.lengths)
         spec.check_rows(int(fwd.shape[1]))
         table = model._lmer_table_for()
         if table is not None:

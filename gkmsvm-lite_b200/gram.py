@@ -14,7 +14,7 @@ import torch
 
 from . import engine
 from ._lib import require_cuda
-from .inputs import as_batch, device_codes
+from .inputs import SeqBatch
 from .kernels import DirectGkmKernel, RbfKernel
 
 _MAX_BLOCK_BYTES = 2 * 2**30
@@ -28,18 +28,15 @@ def compute_gram(kernel, X, Y=None, *, chunk_size=1000, verbose=False, out=None,
     dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
     base = kernel.base
     symmetric = Y is None
-    X, lengths = as_batch(X, lengths)
-    if symmetric:
-        Y, y_lengths = X, lengths
-    else:
-        Y, y_lengths = as_batch(Y, y_lengths)
-    N, M = X.shape[0], Y.shape[0]
+    xb = SeqBatch.read(X, lengths)
+    yb = xb if symmetric else SeqBatch.read(Y, y_lengths)
+    N, M = xb.B, yb.B
     spec = engine.Spec(base, dev)
-    bx, rx, cx = engine.pack(spec, device_codes(X, dev), lengths)
+    bx, rx, cx = engine.pack(spec, xb.on(dev), xb.lengths)
     if symmetric:
         by, ry, cy = bx, rx, cx
     else:
-        by, ry, cy = engine.pack(spec, device_codes(Y, dev), y_lengths)
+        by, ry, cy = engine.pack(spec, yb.on(dev), yb.lengths)
     spec.check_rows(int(max(bx.shape[1], by.shape[1])))
     dx = dy = None
     if base.normalize:

@@ -14,7 +14,7 @@ import warnings
 import numpy as np
 
 from . import _lib
-from .inputs import LSGKM_MAX_LENGTH, as_batch, encode_codes
+from .inputs import LSGKM_MAX_LENGTH, SeqBatch
 from .kernels import KERNEL_ALIASES
 from .model import GkmSVM
 
@@ -181,8 +181,8 @@ def load_classic_model(alpha_path, svseq_path=None, *, L: int = 10, k: int = 6, 
                                   f"supported; use {sorted(GKMSVM_FILTERS)}")
     if not seqs:
         raise ValueError("No support vector sequences found")
-    codes = [encode_codes(s) for s in seqs]
-    sv, lengths = as_batch(codes)
+    svb = SeqBatch.read(seqs)
+    sv, lengths = svb.codes, svb.lengths
     params = {"L": L, "k": k, "d": d, "include_rc": bool(include_rc)}
     return GkmSVM(sv, np.array(coefs, dtype=np.float64), 0.0, GKMSVM_FILTERS[filter_type], params,
                   sv_lengths=lengths, sv_chunk_size=sv_chunk_size, device=device)

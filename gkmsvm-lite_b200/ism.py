@@ -14,7 +14,7 @@ import torch
 
 from . import engine
 from ._lib import call, ptr, stream_handle
-from .inputs import as_batch, device_codes, per_position, rows, short_rows
+from .inputs import SeqBatch, device_codes, per_position
 from .kernels import RbfKernel
 
 # Sequences per device pass: ISM outputs [B, 4, L] float64 per pass within this
@@ -25,10 +25,10 @@ def ism(model, x, *, lengths=None, batch_size=None, verbose=False) -> torch.Tens
     """[B, 4, L] f(mutant) - f(x) for every single-base substitution; 0 past
     each row's length, NaN rows shorter than l (ism.py:21-64)."""
     dev = model._require_gpu()
-    x, lengths = as_batch(x, lengths)
+    batch = SeqBatch.read(x, lengths)
     l = model.kernel.base.l
-    short = short_rows(lengths, l, "ISM deltas")
-    B, L = x.shape
+    short = batch.short(l, "ISM deltas")
+    B, L = batch.B, batch.L
     model._plan_lmer_table(5 * l * B * L)
     bs = batch_size if batch_size is not None else max(1, _BLOCK_BYTES // (8 * 4 * L * 3))
     parts = []
@@ -37,9 +37,10 @@ def ism(model, x, *, lengths=None, batch_size=None, verbose=False) -> torch.Tens
         from tqdm import tqdm
         it = tqdm(it, desc="ISM")
     for s in it:
-        parts.append(_ism_rows(model, x[s:s + bs], rows(lengths, s, bs), dev))
+        p = batch.part(s, bs)
+        parts.append(_ism_rows(model, p.codes, p.lengths, dev))
     out = parts[0] if len(parts) == 1 else torch.cat(parts)
-    return per_position(out, lengths, short)
+    return per_position(out, batch, short)
 
 
 def _ism_rows(model, x, lengths, dev):

@@ -16,8 +16,7 @@ import torch
 
 from . import engine
 from ._lib import require_cuda
-from .inputs import (allele_arrays, as_batch, device_codes, joint_lengths, nan_rows, rows,
-                     short_rows, to_codes, uniform_or_lengths)
+from .inputs import SeqBatch, allele_batches, device_codes, nan_rows, to_codes
 from .kernels import KERNEL_BUILDERS, DirectGkmKernel, RbfKernel, neighbor_count, resolve_kernel_type
 
 # Join-path [rows, S] float64 blocks stay within this (svm.py:475)
@@ -52,7 +51,7 @@ class GkmSVM:
             raise ValueError(f"Number of support sequences ({sv.shape[0]}) must match number of "
                              f"coefficients ({coef.shape[0]})")
         self.support_sequences = sv
-        self.sv_lengths = uniform_or_lengths(sv_lengths, sv.shape)
+        self.sv_lengths = SeqBatch.checked_lengths(sv_lengths, sv.shape)
         self.coefficients = coef.astype(np.float64)
         self.bias = float(bias)
         self.kernel_type = resolve_kernel_type(kernel_type)
@@ -276,33 +275,31 @@ class GkmSVM:
         fwd, rc, counts = engine.pack(self._spec(), xt, lengths)
         return self._score_packed(fwd, rc, counts)
 
-    def _score_unbatched(self, codes, lengths) -> torch.Tensor:
-        B, L = codes.shape
-        W = max(L - self.kernel.l + 1, 1)
+    def _score_unbatched(self, batch: SeqBatch) -> torch.Tensor:
+        W = max(batch.L - self.kernel.l + 1, 1)
         step = max(1, _MAX_PACK_BYTES // (8 * W))
-        parts = [self._score_codes(codes[s:s + step], rows(lengths, s, step)) for s in range(0, B, step)]
+        parts = [self._score_codes(p.codes, p.lengths) for p in (batch.part(s, step) for s in range(0, batch.B, step))]
         return parts[0] if len(parts) == 1 else torch.cat(parts)
 
     def __call__(self, x, *, lengths=None, batch_size=None, verbose=False) -> torch.Tensor:
         """[B, 1] float64 decision values on the model's CUDA device; NaN for
         rows shorter than l (svm.py:407-451)."""
         dev = self._require_gpu()
-        x, lengths = as_batch(x, lengths)
+        batch = x if isinstance(x, SeqBatch) else SeqBatch.read(x, lengths)
         l = self.kernel.l
-        short = short_rows(lengths, l)
-        B = x.shape[0]
+        short = batch.short(l)
+        B = batch.B
         if short is not None and short.all():
             return torch.full((B, 1), float("nan"), dtype=torch.float64, device=dev)
-        self._plan_lmer_table(B * max(x.shape[-1] - l + 1, 0))
+        self._plan_lmer_table(B * max(batch.L - l + 1, 0))
         if batch_size is not None and B > batch_size:
             it = range(0, B, batch_size)
             if verbose:
                 from tqdm import tqdm
                 it = tqdm(it, desc="Scoring")
-            out = torch.cat([self._score_unbatched(x[s:s + batch_size], rows(lengths, s, batch_size))
-                             for s in it])
+            out = torch.cat([self._score_unbatched(batch.part(s, batch_size)) for s in it])
         else:
-            out = self._score_unbatched(x, lengths)
+            out = self._score_unbatched(batch)
         return nan_rows(out[:, None], short)
 
     def score_variants(self, ref, alt, *, method="kernel", ref_lengths=None, alt_lengths=None,
@@ -310,14 +307,9 @@ class GkmSVM:
         """[B, 1] variant effects (svm.py:600-662): score(alt) - score(ref), or
         GkmExplain mutation impact (lsgkm gkmexplain -m 5)."""
         if method == "kernel":
-            ref, alt, ref_lengths, alt_lengths = allele_arrays(ref, alt, ref_lengths, alt_lengths)
-            n = ref.shape[0]
-            both = (torch.cat([torch.as_tensor(alt), torch.as_tensor(ref)])
-                    if isinstance(ref, torch.Tensor) or isinstance(alt, torch.Tensor)
-                    else np.concatenate([alt, ref]))
-            scores = self(both, lengths=joint_lengths(ref.shape[-1], (n, alt_lengths), (n, ref_lengths)),
-                          batch_size=batch_size, verbose=verbose)
-            return scores[:n] - scores[n:]
+            r, a = allele_batches(ref, alt, ref_lengths, alt_lengths)
+            scores = self(SeqBatch.stacked(a, r), batch_size=batch_size, verbose=verbose)
+            return scores[:r.B] - scores[r.B:]
         if method == "gkmexplain":
             from .explain import mutation_impact
 

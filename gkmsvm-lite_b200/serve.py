@@ -302,17 +302,17 @@ class GpuBackend:
         return int(free + max(cached, 0))
 
     def prepare(self, r: Request):
-        from .inputs import allele_arrays, as_batch
+        from .inputs import SeqBatch, allele_batches
 
         if r.kind == "score_variants":
-            ref, alt, rl, al = allele_arrays(r.x, r.alt, r.lengths, r.alt_lengths)
-            r.x, r.alt, r.lengths, r.alt_lengths = ref, alt, rl, al
-            n, L = ref.shape
+            rb, ab = allele_batches(r.x, r.alt, r.lengths, r.alt_lengths)
+            r.x, r.alt, r.lengths, r.alt_lengths = rb.codes, ab.codes, rb.lengths, ab.lengths
+            n, L = rb.B, rb.L
             r.rows = 2 * n
         else:
-            x, ln = as_batch(r.x, r.lengths)
-            r.x, r.lengths = x, ln
-            n, L = x.shape
+            b = SeqBatch.read(r.x, r.lengths)
+            r.x, r.lengths = b.codes, b.lengths
+            n, L = b.B, b.L
             r.rows = n
         # packed windows + scratch of its rows (ISM: mutant window sets too)
         # device memory while it runs: packed windows and float64 outputs; an

@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib, engine
-from .inputs import as_batch, device_codes
+from .inputs import SeqBatch
 from .kernels import DirectGkmKernel, RbfKernel
 
 # most columns computed per column-cache miss: the requested one plus the
@@ -41,10 +41,10 @@ class KernelColumnCache:
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.kernel = kernel
         base = kernel.base
-        X, lengths = as_batch(X, lengths)
-        self.N = X.shape[0]
+        xb = SeqBatch.read(X, lengths)
+        self.N = xb.B
         self.spec = engine.Spec(base, dev)
-        self.fwd, self.rc, self.counts = engine.pack(self.spec, device_codes(X, dev), lengths)
+        self.fwd, self.rc, self.counts = engine.pack(self.spec, xb.on(dev), xb.lengths)
         self.spec.check_rows(int(self.fwd.shape[1]))
         self.diag = (engine.self_kernel(self.spec, self.fwd, self.rc, self.counts) if base.normalize
                      else torch.ones(self.N, dtype=torch.float64, device=dev))

@@ -92,11 +92,38 @@ def test_as_batch_strings_and_one_hot():
     assert inputs.as_batch(np.zeros((2, 5), np.uint8), lengths=[5, 5])[1] is None
 
 
-def test_allele_arrays_pad_indels():
-    ref, alt, rl, al = inputs.allele_arrays(["ACGTA"], ["ACGTAAC"])
-    assert ref.shape == alt.shape == (1, 7)
-    np.testing.assert_array_equal(rl, [5])
-    assert al is None
+def test_allele_batches_pad_indels():
+    ref, alt = inputs.allele_batches(["ACGTA"], ["ACGTAAC"])
+    assert ref.codes.shape == alt.codes.shape == (1, 7)
+    np.testing.assert_array_equal(ref.lengths, [5])
+    np.testing.assert_array_equal(alt.lengths, [7])
+
+
+def test_seq_batch_rows_and_masks():
+    import torch
+
+    b = inputs.SeqBatch.read(["ACGTACGTACGT", "ACG", "TTTTTTTTTTTTTT"])
+    assert (b.B, b.L) == (3, 14)
+    np.testing.assert_array_equal(b.lengths, [12, 3, 14])
+    assert b.n_windows(11) == 2 + 0 + 4
+    with pytest.warns(UserWarning, match="fewer than l = 11"):
+        short = b.short(11)
+    np.testing.assert_array_equal(short, [False, True, False])
+    p = b.part(1, 2)
+    np.testing.assert_array_equal(p.lengths, [3, 14])
+    both = inputs.SeqBatch.stacked(b.part(0, 1), b.part(2, 1))
+    np.testing.assert_array_equal(both.lengths, [12, 14])
+    out = torch.ones((3, 4, 14), dtype=torch.float64)
+    m = inputs.per_position(out, b, short)
+    assert torch.isnan(m[1]).all()
+    assert m[0, :, :12].eq(1).all() and m[0, :, 12:].eq(0).all()
+    assert m[2].eq(1).all()
+    with pytest.raises(ValueError):
+        inputs.encode_codes("ACGN")
+    np.testing.assert_array_equal(inputs.encode_codes("ACGN", allow_n=True), [0, 1, 2, 0])
+    with pytest.raises(ValueError):
+        inputs.encode_codes("ACGX", allow_n=True)
+    np.testing.assert_array_equal(inputs.encode_codes("acgx", allow_other=True), [0, 1, 2, 0])
 
 
 def test_model_on_cpu_refuses_to_compute():
