@@ -10,8 +10,11 @@ batches against full SV replicas (weak scaling, no collective on the data
 path); the time is the max over ranks.  Rank 0 prints one JSON line.
 
 --impl reference times the CPU restatement of the reference's index path
-(oracle/gkm_oracle.c, pthreads over all host cores) on a bounded sample of the
-same workload.
+(oracle/gkm_oracle.c, pthreads over all host cores, rows handed out one at a
+time) on bounded samples of the same query stream rank 0 scores.
+
+With --gpus N > 1 and no torchrun environment, the script starts N ranks
+itself under torch.distributed.run; under torchrun, WORLD_SIZE must equal N.
 """
 
 from __future__ import annotations
@@ -34,6 +37,74 @@ PARAMS_T3 = {"L": 11, "k": 7, "d": 3, "gamma": 2.0}
 PARAMS_T2 = {"L": 11, "k": 7, "d": 3}
 WORKLOAD = ("config3: 72,000 SVs (200-500 bp, alpha ~ N(0, 0.1^2)), t=3 gkmrbf gamma=2, "
             "queries 50-2000 bp log-uniform with 0.5% N")
+
+
+def job_config(queries: int, world: int) -> dict:
+    """The workload description both arms print (the same dict for both)."""
+    return {"workload": WORKLOAD, "queries_per_rank": queries, "svs": 72000, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (100k packed queries: 1.6 GB; the 148 MB SV index also exceeds the 126 MB L2)"}
+
+
+def shard_seed(rank: int, base: int = 102) -> int:
+    """Each rank scores its own query batch: the config-3 stream of seed base + rank."""
+    return base + rank
+
+
+def launch_command(args, env) -> list[str] | None:
+    """The torchrun command that starts --gpus ranks when this process is not
+    a rank of one already (None: run here).  Raises when a torchrun world
+    disagrees with --gpus."""
+    world = env.get("WORLD_SIZE")
+    if world is not None:
+        if int(world) != args.gpus:
+            raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; launch one rank per GPU")
+        return None
+    if args.gpus <= 1:
+        return None
+    import socket
+
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+
+
+def timed_region(step, steps: int, warmup: int, dist=None, sync=lambda: None, clock=None) -> float:
+    """warmup untimed steps, then `steps` timed steps bracketed by a barrier and
+    a device sync on both sides; this rank's seconds.  clock: a (start, stop)
+    pair of callables returning seconds (default perf_counter); the GPU arm
+    passes CUDA events."""
+    for _ in range(warmup):
+        step()
+    sync()
+    if dist is not None:
+        dist.barrier()
+    sync()
+    if clock is None:
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            step()
+        sync()
+        return time.perf_counter() - t0
+    start, stop = clock
+    start()
+    for _ in range(steps):
+        step()
+    return stop()
+
+
+def job_throughput(seconds: float, units: float, dist=None, device=None) -> tuple[float, float, float]:
+    """(max seconds over ranks, units summed over ranks, whole-job units/s)."""
+    if dist is not None:
+        import torch
+
+        t = torch.tensor([seconds, float(units)], dtype=torch.float64, device=device)
+        tmax, tsum = t[:1].clone(), t[1:].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        seconds, units = float(tmax.item()), float(tsum.item())
+    return seconds, units, units / seconds
 
 
 def parse():
@@ -99,96 +170,90 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def events_time(fn, stream=None):
-    import torch
-
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    out = fn()
-    b.record()
-    return a, b, out
 
 
-def cpu_baseline(model_np, sv_diag, xq, xl, kind_params, budget_s=15.0):
-    """The oracle's C restatement of the reference index path, all host threads,
-    on a sample sized to about budget_s."""
-    from oracle import oracle as orc
+class PortBaseline:
+    """The oracle's C restatement of the reference's CPU index path (SV l-mer
+    index, fused query + RBF + alpha reduce, query self-kernels) on every host
+    thread, rows handed out one at a time.  Built once per process: the index
+    and the SV self-kernels are the model caches the reference builds on its
+    first call."""
 
-    sv, svl, coef = model_np
-    kd = orc.KernelDef.from_params("gkmrbf", kind_params)
-    m = orc.OracleModel(sv, svl, coef, 0.0, kd)
-    ib = orc.IndexBaseline(m, sv_diag=sv_diag)
-    threads = os.cpu_count() or 1
-    n = 16
-    t0 = time.perf_counter()
-    ib.scores(xq[:n, : int(xl[:n].max())], xl[:n], threads=threads)
-    t1 = time.perf_counter() - t0
-    per = t1 / n
-    n2 = int(min(len(xl), max(n, budget_s / max(per, 1e-9))))
-    L = int(xl[:n2].max())
-    t0 = time.perf_counter()
-    ib.scores(xq[:n2, :L], xl[:n2], threads=threads)
-    dt = time.perf_counter() - t0
-    return {"value": n2 / dt, "unit": "seqs/sec", "cores": threads, "kind": "port",
-            "sample": f"{n2} config-3 queries (t=3), steady state (SV index and self-kernels built)",
-            "seconds": dt}
+    def __init__(self, sv, svl, coef):
+        from oracle import oracle as orc
+
+        self.threads = os.cpu_count() or 1
+        kd = orc.KernelDef.from_params("gkmrbf", PARAMS_T3)
+        t0 = time.perf_counter()
+        self.ib = orc.IndexBaseline(orc.OracleModel(sv, svl, coef, 0.0, kd), threads=self.threads)
+        self.build_s = time.perf_counter() - t0
+
+    def scores(self, xq, xl, rows) -> np.ndarray:
+        rows = np.asarray(rows)
+        L = int(xl[rows].max())
+        return self.ib.scores(xq[rows, :L], xl[rows], threads=self.threads)[:, 0]
+
+    def time_rows(self, xq, xl, rows) -> float:
+        t0 = time.perf_counter()
+        self.scores(xq, xl, rows)
+        return time.perf_counter() - t0
+
+
+# rows of the query stream each reference-arm step times (and the cpu_baseline
+# sample of the GPU arm): consecutive, so every length in the stream's mix
+REF_ROWS_PER_STEP = 320
+
+
+def parity_rows(xl, nmask, n=256, seed=7) -> np.ndarray:
+    """Rows of a timed batch the oracle re-scores: the 16 longest, the 16 with
+    the largest share of N bases, and random others."""
+    nfrac = nmask.sum(axis=1) / np.maximum(xl, 1)
+    pick = list(np.argsort(-xl, kind="stable")[:16]) + list(np.argsort(-nfrac, kind="stable")[:16])
+    rest = np.setdiff1d(np.arange(len(xl)), pick)
+    pick += list(np.random.default_rng(seed).choice(rest, n - len(set(pick)), replace=False))
+    return np.unique(np.asarray(pick))
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     import gkmsvm_lite_b200.synthetic as syn
-    from oracle import oracle as orc
 
     sv, svl, coef = syn.config3_model()
-    xq, xl, _ = syn.config3_queries(n=min(args.queries, 20000))
-    kd = orc.KernelDef.from_params("gkmrbf", PARAMS_T3)
-    m = orc.OracleModel(sv, svl, coef, 0.0, kd)
-    # SV self-kernels: a model cache the reference builds once (not timed)
+    # the same stream rank 0 of the GPU arm scores
+    xq, xl, _ = syn.config3_queries(seed=shard_seed(0), n=args.queries)
     t0 = time.perf_counter()
-    ds = _sv_diag_threaded(sv, svl, kd)
-    build_s = time.perf_counter() - t0
-    ib = orc.IndexBaseline(m, sv_diag=ds)
-    threads = os.cpu_count() or 1
-    per_step = 32
-    for _ in range(args.warmup):
-        ib.scores(xq[:8, : int(xl[:8].max())], xl[:8], threads=threads)
+    base = PortBaseline(sv, svl, coef)
+    first_rows = np.arange(REF_ROWS_PER_STEP)
+    base.time_rows(xq, xl, first_rows)
+    first_s = time.perf_counter() - t0  # caches built + the first call
+    nsteps = max(1, (len(xl) - REF_ROWS_PER_STEP) // REF_ROWS_PER_STEP)
     times = []
-    for s in range(args.steps):
-        lo = (s * per_step) % (len(xl) - per_step)
-        sl = slice(lo, lo + per_step)
-        L = int(xl[sl].max())
-        t0 = time.perf_counter()
-        ib.scores(xq[sl, :L], xl[sl], threads=threads)
-        times.append(time.perf_counter() - t0)
-    v = per_step * len(times) / sum(times)
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "seqs/sec", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+
+    def step(k=[0]):
+        lo = REF_ROWS_PER_STEP * (1 + k[0] % nsteps)
+        times.append(base.time_rows(xq, xl, np.arange(lo, lo + REF_ROWS_PER_STEP)))
+        k[0] += 1
+
+    for _ in range(args.warmup):  # small calls, as the reference's own benchmark warms up
+        base.time_rows(xq, xl, np.arange(8))
+    total = timed_region(step, args.steps, 0)
+    v = REF_ROWS_PER_STEP * args.steps / total
+    sample = (f"{REF_ROWS_PER_STEP} consecutive queries of the seed-{shard_seed(0)} stream per step "
+              f"(steady state); first call {first_s:.1f} s (SV index {base.build_s:.1f} s with the SV "
+              f"self-kernels, then {REF_ROWS_PER_STEP} queries)")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "seqs/sec", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "queries_per_step": per_step},
-            "cpu_baseline": {"value": v, "unit": "seqs/sec", "cores": threads, "kind": "port",
-                             "sample": f"{per_step} queries per step (t=3), SV caches built first "
-                                       f"({build_s:.1f} s, untimed)"},
+            "data": "synthetic", "config": job_config(args.queries, world),
+            "cpu_baseline": {"value": v, "unit": "seqs/sec", "cores": base.threads, "kind": "port",
+                             "sample": sample, "first_s": first_s,
+                             "steady_s_per_step": float(np.mean(times))},
             "e2e": {"value": v, "unit": "seqs/sec", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
-
-
-def _sv_diag_threaded(sv, svl, kd):
-    """K(sv, sv) of every SV with the oracle, split over host threads."""
-    from concurrent.futures import ThreadPoolExecutor
-
-    from oracle import oracle as orc
-
-    n = os.cpu_count() or 1
-    parts = np.array_split(np.arange(len(sv)), max(1, n * 4))
-
-    def one(ix):
-        return orc.raw_from_profiles(orc.self_profiles(sv[ix], svl[ix], kd), kd)
-
-    with ThreadPoolExecutor(n) as ex:
-        return np.concatenate(list(ex.map(one, parts)))
 
 
 def serving_leg(sv, svl, coef, n_requests=600, seed=4):
@@ -516,7 +581,7 @@ def run_b200(args):
     dev = torch.device("cuda", local)
 
     sv, svl, coef = syn.config3_model()
-    xq, xl, _ = syn.config3_queries(seed=102 + rank, n=args.queries)
+    xq, xl, nmask = syn.config3_queries(seed=shard_seed(rank), n=args.queries)
     model = gk.GkmSVM(sv, coef, 0.0, "gkmrbf", PARAMS_T3, sv_lengths=svl).cuda()
     model.use_lmer_table = False
     t0 = time.perf_counter()
@@ -524,7 +589,6 @@ def run_b200(args):
     torch.cuda.synchronize()
     index_build_s = time.perf_counter() - t0
     spec = model._spec()
-    inv_ds, svcoef = model._inv_ds(), model._sv_coef()
     x_dev = torch.from_numpy(xq).to(dev)
     l_dev = torch.from_numpy(xl).to(dev)
     B = x_dev.shape[0]
@@ -533,42 +597,42 @@ def run_b200(args):
 
     scorer = BatchedScorer(model)
     query_ev = []
+    last = {}
 
     def step():
         e = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-        out = scorer.score(x_dev, l_dev, events=e, check=False)
+        last["scores"] = scorer.score(x_dev, l_dev, events=e, check=False)
         query_ev.append(e)
-        return out
 
-    for _ in range(args.warmup):
-        step()
-    scorer.check_flags()
-    torch.cuda.synchronize()
-    query_ev.clear()
-    if dist is not None:
-        dist.barrier()
+    def warm():
+        for _ in range(args.warmup):
+            step()
+        scorer.check_flags()
+        query_ev.clear()
+
+    warm()
     before = index.counters()
     torch.cuda.synchronize()
-    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clocks:
-        t_start.record()
-        for _ in range(args.steps):
-            scores = step()
-        t_end.record()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def stop():
+        ev1.record()
         torch.cuda.synchronize()
-    elapsed = t_start.elapsed_time(t_end) / 1e3
+        return ev0.elapsed_time(ev1) / 1e3
+
+    with Clocks(local) as clocks:
+        elapsed = timed_region(step, args.steps, 0, dist=dist, sync=torch.cuda.synchronize,
+                               clock=(ev0.record, stop))
+    elapsed, units, value = job_throughput(elapsed, args.steps * B, dist=dist, device=dev)
     if dist is not None:
-        t = torch.tensor([elapsed], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
         dist.barrier()
     after = index.counters()
     torch.cuda.synchronize()
     # 16-bit counter carries never outgrew a block's log in the timed steps
     counts_exact = int(after[0]) == int(before[0]) and int(after[1]) == int(before[1])
     per_step = elapsed / args.steps
-    value = world * B / per_step
     query_ms = float(np.mean([a.elapsed_time(b) for a, b in query_ev]))
+    timed_scores = last["scores"].cpu().numpy().copy()
 
     result = None
     if rank == 0:
@@ -586,12 +650,12 @@ def run_b200(args):
         lookups = n_win * int(index.masks.numel())
         entry_bytes = 2 if (not spec.base.weighted and index.tile_svs <= 65536) else 4
         alg_bytes = lookups * 8 + hits * entry_bytes + 12 * n_win
+        alg_bytes_4b = lookups * 8 + hits * 4 + 12 * n_win  # the 4-byte-id count
         # DRAM traffic of the launch: ncu's dram__bytes_read.sum +
         # dram__bytes_write.sum on a 2,000-query launch of this workload
         # (1.4475e9 B; the SV index stays in L2), scaled by queries
         traffic = 1.4475e9 * B / 2000
-        score_ms = query_ms
-        achieved = alg_bytes / (score_ms / 1e3) / 1e9
+        achieved = alg_bytes / (query_ms / 1e3) / 1e9
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -602,16 +666,18 @@ def run_b200(args):
             "metric": METRIC, "value": value, "unit": "seqs/sec", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32 counts + f64 epilogue", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "queries_per_rank": B, "svs": len(coef), "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (100k packed queries: 1.6 GB; the 148 MB SV index also exceeds the 126 MB L2)"},
+            "config": job_config(B, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "traffic_source": "ncu dram bytes of a 2,000-query launch, scaled by queries",
                          "kernel": "index_query (fused SV-tile query + RBF + alpha reduce)",
                          "alg_bytes_per_launch": alg_bytes, "hits": hits, "lookups": lookups,
+                         "frac_4byte_ids": alg_bytes_4b / (query_ms / 1e3) / 1e9 / peak,
+                         "binding_unit": "L1/shared-memory atomics and L2 gathers (the index is L2-resident; "
+                                         "see l1tex / lts throughput in the ncu summary)",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6.65 TB/s"},
-            "stages_ms": {"prep (pack, self-kernels, order)": per_step * 1e3 - score_ms,
-                          "index_query + finish": score_ms},
+            "stages_ms": {"prep (pack, self-kernels, order)": per_step * 1e3 - query_ms,
+                          "index_query + finish": query_ms},
             "form": "batched: CUDA-graph replay of pack + self-kernel + persistent work-queue index query",
             "index": {"build_s": index_build_s, "entries": index.entries, "tiles": index.tiles,
                       "tile_svs": index.tile_svs, "device_MB": index.nbytes / 1e6},
@@ -634,7 +700,7 @@ def run_b200(args):
         host_scores = model(xh, lengths=lh).cpu().numpy()
         b.record()
         torch.cuda.synchronize()
-        e2e_s = a.elapsed_time(b) / 1e3
+        e2e_s, e2e_n, e2e_v = job_throughput(a.elapsed_time(b) / 1e3, nq, dist=dist, device=dev)
         plain_n = min(nq, 5000)
         a.record()
         for s in range(0, plain_n, 1000):
@@ -643,8 +709,8 @@ def run_b200(args):
         torch.cuda.synchronize()
         plain_s = a.elapsed_time(b) / 1e3
         if rank == 0:
-            result["e2e"] = {"value": nq / e2e_s, "unit": "seqs/sec", "h2d_bytes_per_step": int(xh.nbytes + lh.nbytes),
-                             "d2h_bytes_per_step": int(host_scores.nbytes), "queries": nq}
+            result["e2e"] = {"value": e2e_v, "unit": "seqs/sec", "h2d_bytes_per_step": int(xh.nbytes + lh.nbytes),
+                             "d2h_bytes_per_step": int(host_scores.nbytes), "queries_per_rank": nq}
             result["plain_per_call"] = {"value": plain_n / plain_s, "unit": "seqs/sec", "calls_of": 1000,
                                         "note": "model(x) per 1,000-query call with host inputs and output"}
             result["batched_vs_plain"] = value / world / result["plain_per_call"]["value"]
@@ -664,15 +730,35 @@ def run_b200(args):
             torch.cuda.synchronize()
             result["t2_table"] = {"value": 3 * B / (a.elapsed_time(b) / 1e3), "unit": "seqs/sec",
                                   "table_build_s": tb}
+            del m2
             if world == 1:
                 result["serving"] = serving_leg(sv, svl, coef)
                 result["ism_explain"] = ism_explain_leg(sv, svl, coef)
                 result["deltasvm"] = deltasvm_leg(sv, svl, coef)
                 result["gram"] = gram_leg(args.gram_n)
                 result["training"] = training_leg(args.gram_n)
-                result["cpu_baseline"] = cpu_baseline((sv, svl, coef), model._sv_diag().cpu().numpy(), xq, xl,
-                                                      PARAMS_T3)
     if rank == 0:
+        # the oracle re-scores rows of the timed batch (the longest, the most
+        # N-heavy, random others) and, at N=1, times the reference's CPU path
+        port = PortBaseline(sv, svl, coef)
+        rows = parity_rows(xl, nmask)
+        want = port.scores(xq, xl, rows)
+        got = timed_scores[rows]
+        rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-300)
+        result["parity"] = {"rows": int(len(rows)), "of": "the last timed step's scores",
+                            "max_rel_err": float(rel.max()), "max_abs_err": float(np.abs(got - want).max()),
+                            "rtol": 1e-9, "atol": 1e-12,
+                            "pass": bool(np.all(np.abs(got - want) <= 1e-12 + 1e-9 * np.abs(want))),
+                            "longest_row_bp": int(xl[rows].max())}
+        if world == 1 and not args.no_extras:
+            sample = np.arange(REF_ROWS_PER_STEP, 2 * REF_ROWS_PER_STEP)
+            port.time_rows(xq, xl, np.arange(8))
+            sec = port.time_rows(xq, xl, sample)
+            result["cpu_baseline"] = {"value": len(sample) / sec, "unit": "seqs/sec", "cores": port.threads,
+                                      "kind": "port", "seconds": sec,
+                                      "sample": f"{len(sample)} consecutive config-3 queries (rows "
+                                                f"{sample[0]}..{sample[-1]} of the timed batch), steady state "
+                                                f"(SV index and self-kernels built)"}
         result.setdefault("e2e", None)
         print(json.dumps(result), flush=True)
     if dist is not None:
@@ -683,6 +769,9 @@ def run_b200(args):
 
 def main():
     args = parse()
+    cmd = launch_command(args, os.environ)
+    if cmd is not None:
+        return subprocess.call(cmd)
     if args.impl == "reference":
         return run_reference(args)
     if args.leg == "gram":

@@ -929,6 +929,7 @@ extern "C" int gkm_index_score(const gkm_index_t *ix, const uint32_t *bx, const 
 {
     if (!ix || !bx || !cx || !inv_dx || !inv_ds || !coef || !scores)
         return gkm_fail(GKM_ERR_INVALID, "null argument");
+    if (B < 0 || W < 1) return gkm_fail(GKM_ERR_INVALID, "rows %lld, windows per row %lld", (long long)B, (long long)W);
     if (B == 0) return GKM_OK;
     cudaStream_t st = (cudaStream_t)stream;
     double *partial = nullptr;
@@ -1191,6 +1192,9 @@ static __device__ __align__(256) double g_noalloc_partials[GKM_NOALLOC_MAX_PARTI
 // Device address of g_noalloc_partials on the current device.  In host code
 // the array's name is only a host-side stand-in, so the address comes from
 // cudaGetSymbolAddress, once per device (with that device current), cached.
+// The cache lives as long as the device's context: a process that calls
+// cudaDeviceReset must not call gkm_index_score_noalloc on that device again
+// (the cached address would belong to the destroyed context).
 static int noalloc_partials(double **out)
 {
     static std::mutex mu;
@@ -1219,6 +1223,9 @@ extern "C" int gkm_index_score_noalloc(const gkm_index_t *ix, const uint32_t *bx
 {
     if (!ix || !bx || !cx || !inv_dx || !inv_ds || !coef || !scores)
         return gkm_fail(GKM_ERR_INVALID, "null argument");
+    if (B < 0 || W < 1)
+        return gkm_fail(GKM_ERR_INVALID, "gkm_index_score_noalloc: rows %lld, windows per row %lld", (long long)B,
+                        (long long)W);
     if (B == 0) return GKM_OK;
     if (B * (int64_t)ix->tiles > GKM_NOALLOC_MAX_PARTIALS)
         return gkm_fail(GKM_ERR_CAPACITY,

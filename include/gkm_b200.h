@@ -141,9 +141,15 @@ int gkm_index_score(const gkm_index_t *index, const uint32_t *bx, const int32_t 
  * 4 MiB device array that the library holds on every device it is loaded on
  * until exit, so B x tiles must be <= 524,288 (GKM_ERR_CAPACITY otherwise).
  * The first call on a device looks that array's address up
- * (cudaGetSymbolAddress): make it before any stream capture.  All calls share
- * the array, so calls that overlap on the GPU (other streams, other threads)
- * race; serialise them. */
+ * (cudaGetSymbolAddress): make it before any stream capture.  The address is
+ * kept for the life of the device's context: do not call this again on a
+ * device after cudaDeviceReset.  All calls share the array, so calls that
+ * overlap on the GPU (other streams, other threads) race; serialise them.
+ * Exactness, as for gkm_index_score: unweighted indexes count in 16-bit fields
+ * with a per-block carry log; a block whose log overflows only raises event
+ * count [0] of gkm_index_status, so a caller that needs exact scores reads
+ * those counts before and after the call and, if [0] moved, rescores with
+ * 32-bit counters (gkm_index_status wide = 1). */
 int gkm_index_score_noalloc(const gkm_index_t *index, const uint32_t *bx, const int32_t *cx,
                             int64_t B, int64_t W, const double *inv_dx, const double *inv_ds,
                             const double *coef, double gamma, int32_t rbf, double bias,

@@ -129,12 +129,47 @@ void orc_self_profiles(const uint32_t *fwd, const uint32_t *rc, const uint8_t *w
     }
 }
 
+typedef struct {
+    const uint32_t *fwd, *rc;
+    const uint8_t *w;
+    int64_t B, W;
+    int l;
+    uint64_t *out;
+    int64_t *next_row;
+} self_job;
+
+static void *self_worker(void *arg)
+{
+    self_job *j = (self_job *)arg;
+    for (;;) {
+        int64_t b = __atomic_fetch_add(j->next_row, 1, __ATOMIC_RELAXED);
+        if (b >= j->B) break;
+        orc_self_profiles(j->fwd + b * j->W, j->rc ? j->rc + b * j->W : NULL, j->w ? j->w + b * j->W : NULL, 1,
+                          j->W, j->l, j->out + b * (j->l + 1));
+    }
+    return NULL;
+}
+
+/* orc_self_profiles over nthreads threads, rows handed out one at a time. */
+void orc_self_profiles_mt(const uint32_t *fwd, const uint32_t *rc, const uint8_t *w,
+                          int64_t B, int64_t W, int l, uint64_t *out, int nthreads)
+{
+    if (nthreads < 1) nthreads = 1;
+    int64_t next_row = 0;
+    self_job j = {fwd, rc, w, B, W, l, out, &next_row};
+    pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * nthreads);
+    for (int t = 0; t < nthreads; t++) pthread_create(&th[t], NULL, self_worker, &j);
+    for (int t = 0; t < nthreads; t++) pthread_join(th[t], NULL);
+    free(th);
+}
+
 /* ------------------------------------------------------------------------ */
 /* l-mer index and fused query + reduce: the reference CPU path that the bench
  * times as its baseline (kernels/lmer_index.py:161-200 build;
  * kernels/lmer_index_cpu.py:11-19 _counting_sort, :23-37 _add_window,
- * :71-120 _query_reduce_cpu).  Threads: pthreads over rows, one length-S
- * accumulator per thread, zeroed as it is reduced. */
+ * :71-120 _query_reduce_cpu).  Threads: pthreads taking rows one at a time
+ * from a shared counter (as a parallel loop with dynamic scheduling would),
+ * one length-S accumulator per thread, zeroed as it is reduced. */
 
 typedef struct {
     int l;
@@ -226,10 +261,7 @@ typedef struct {
     double gamma;
     int rbf;
     double *out;
-    /* raw mode */
-    double *raw;
-    int64_t diag_offset;
-    int nthreads, tid;
+    int64_t *next_row; /* shared: rows are handed out one at a time */
 } reduce_job;
 
 static void *reduce_worker(void *arg)
@@ -238,7 +270,9 @@ static void *reduce_worker(void *arg)
     int64_t S = j->ix->S;
     double *acc = (double *)calloc(S ? S : 1, sizeof(double));
     double floor_ = j->rbf ? exp(-j->gamma) : 1.0;
-    for (int64_t b = j->tid; b < j->B; b += j->nthreads) {
+    for (;;) {
+        int64_t b = __atomic_fetch_add(j->next_row, 1, __ATOMIC_RELAXED);
+        if (b >= j->B) break;
         for (int64_t i = 0; i < j->W; i++) {
             double a = j->wx ? (double)j->wx[b * j->W + i] : 1.0;
             add_window(j->ix, acc, j->bx[b * j->W + i], a, j->masks, j->weights, j->nm, 0);
@@ -272,17 +306,13 @@ void orc_index_reduce(void *p, const uint32_t *bx, const uint8_t *wx, int64_t B,
                       double gamma, int rbf, double *out, int nthreads)
 {
     if (nthreads < 1) nthreads = 1;
+    int64_t next_row = 0;
     pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * nthreads);
-    reduce_job *jobs = (reduce_job *)malloc(sizeof(reduce_job) * nthreads);
-    for (int t = 0; t < nthreads; t++) {
-        reduce_job j = {(orc_index *)p, bx, B, W, wx, masks, weights, nm,
-                        inv_dx, inv_ds, coef, gamma, rbf, out, NULL, -1, nthreads, t};
-        jobs[t] = j;
-        pthread_create(&th[t], NULL, reduce_worker, &jobs[t]);
-    }
+    reduce_job j = {(orc_index *)p, bx, B, W, wx, masks, weights, nm,
+                    inv_dx, inv_ds, coef, gamma, rbf, out, &next_row};
+    for (int t = 0; t < nthreads; t++) pthread_create(&th[t], NULL, reduce_worker, &j);
     for (int t = 0; t < nthreads; t++) pthread_join(th[t], NULL);
     free(th);
-    free(jobs);
 }
 
 /* K_raw [B, S] through the index (kernels/lmer_index_cpu.py:41-67), one row at

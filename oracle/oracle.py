@@ -61,6 +61,7 @@ def lib():
         L.orc_pack.argtypes = [P, P, I64, I64, I, P, P]
         L.orc_profiles.argtypes = [P, P, I64, I64, P, P, I64, I64, I, P]
         L.orc_self_profiles.argtypes = [P, P, P, I64, I64, I, P]
+        L.orc_self_profiles_mt.argtypes = [P, P, P, I64, I64, I, P, I]
         L.orc_index_build.argtypes = [P, P, P, P, I64, I64, I]
         L.orc_index_build.restype = P
         L.orc_index_free.argtypes = [P]
@@ -262,13 +263,17 @@ def profiles(xc, xl, yc, yl, kd: KernelDef) -> np.ndarray:
     return out
 
 
-def self_profiles(xc, xl, kd: KernelDef) -> np.ndarray:
+def self_profiles(xc, xl, kd: KernelDef, threads: int = 1) -> np.ndarray:
     fx, rx = pack(xc, xl, kd.l)
     w = row_weights(fx, kd)
     B, W = fx.shape
     out = np.zeros((B, kd.l + 1), np.uint64)
-    lib().orc_self_profiles(_p(fx), _p(rx if kd.include_rc else None), _p(w), B, W,
-                            kd.l, _p(out))
+    if threads > 1:
+        lib().orc_self_profiles_mt(_p(fx), _p(rx if kd.include_rc else None), _p(w), B, W,
+                                   kd.l, _p(out), int(threads))
+    else:
+        lib().orc_self_profiles(_p(fx), _p(rx if kd.include_rc else None), _p(w), B, W,
+                                kd.l, _p(out))
     return out
 
 
@@ -577,7 +582,7 @@ class IndexBaseline:
     CSR over the SVs' windows (kernels/lmer_index.py:161-200) and the fused
     query + reduce (kernels/lmer_index_cpu.py:71-120)."""
 
-    def __init__(self, model: OracleModel, sv_diag=None):
+    def __init__(self, model: OracleModel, sv_diag=None, threads: int = 1):
         kd = model.kd
         self.kd = kd
         self.model = model
@@ -597,7 +602,7 @@ class IndexBaseline:
         self.masks, lev = neighbor_masks(kd.l, kd.h, kd.dmax)
         self.weights = kd.h[lev].astype(np.float64)
         ds = sv_diag if sv_diag is not None else raw_from_profiles(
-            self_profiles(model.sv, model.sv_lengths, kd), kd)
+            self_profiles(model.sv, model.sv_lengths, kd, threads), kd)
         self.inv_ds = 1.0 / np.sqrt(np.clip(ds, 1e-20, None))
 
     def __del__(self):
@@ -609,7 +614,7 @@ class IndexBaseline:
         kd = self.kd
         fx, _ = pack(xc, xl, kd.l)
         wx = row_weights(fx, kd)
-        dx = diag_x if diag_x is not None else raw_from_profiles(self_profiles(xc, xl, kd), kd)
+        dx = diag_x if diag_x is not None else raw_from_profiles(self_profiles(xc, xl, kd, threads), kd)
         inv_dx = 1.0 / np.sqrt(np.clip(dx, 1e-20, None))
         B, W = fx.shape
         out = np.zeros(B)

@@ -2,7 +2,8 @@
 
 Run in a container that has the reference source tree (never on a GPU box):
 
-    NUMBA_CACHE_DIR=/tmp/nbcache python tests/golden/make_golden.py [groups...]
+    GKMSVM_LITE_ROOT=<gkmsvm-lite checkout> NUMBA_CACHE_DIR=/tmp/nbcache \
+        python tests/golden/make_golden.py [groups...]
 
 groups: small (every kernel type on small ragged inputs: raw kernel values,
 self-kernels, scores, ISM, GkmExplain in three modes, variant scores, mutation
@@ -25,8 +26,11 @@ import time
 
 import numpy as np
 
-REF_SRC = "/root/reference/src"
-REF_FIXTURES = "/root/reference/tests/fixtures"
+# the gkmsvm-lite source tree: GKMSVM_LITE_ROOT, else the read-only mount of
+# the container the fixtures were made in
+REF_ROOT = os.environ.get("GKMSVM_LITE_ROOT", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "src")
+REF_FIXTURES = os.path.join(REF_ROOT, "tests", "fixtures")
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 sys.path.insert(0, REF_SRC)
