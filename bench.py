@@ -115,7 +115,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--queries", type=int, default=100000)
     ap.add_argument("--no-extras", action="store_true", help="skip t=2, plain-call and CPU legs")
-    ap.add_argument("--leg", default="all", choices=["all", "gram", "train", "explain", "explain-pairs", "serve"],
+    ap.add_argument("--leg", default="all",
+                    choices=["all", "gram", "train", "explain", "explain-pairs", "serve", "encode", "pairwise-forms"],
                     help="gram / train / explain: run only the Gram-matrix, SMO training or config-4 ISM and "
                          "GkmExplain leg (one GPU), print its JSON")
     ap.add_argument("--gram-n", type=int, default=4000, help="sequences of the Gram-matrix leg")
@@ -458,6 +459,108 @@ def explain_pairs_leg(n_sv=2000, sv_len=300, rows=100, row_len=300, seed=9):
             "value": rows / s, "unit": "seqs/sec", "window_pairs_per_s": pairs / s}
 
 
+ENCODE_MODEL = os.path.join(ROOT, "tests", "golden", "lsgkm", "encode_ENCFF579AOX.model.txt.gz")
+# the reference's published steady-state seq/s for this shape (1,000 x 300 bp,
+# 72,145 SVs), L40S / A100
+ENCODE_PUBLISHED = {"t2": {"L40S": 45682, "A100": 35160}, "t3": {"L40S": 2202, "A100": 2261}}
+
+
+def encode_leg(n=1000, L=300, seed=6):
+    """The reference's scoring-throughput benchmark shape (its
+    benchmarks/throughput_sweep.py): the 72,145-SV ENCODE model read by the
+    native LS-GKM parser, as t2 (the file's gkm_esttrunc, default path: the
+    l-mer table) and with the same SVs as gkmrbf gamma=1 (t3, the l-mer index);
+    n synthetic L bp queries as host one-hot [n, 4, L]; model(X) read back to
+    the host, timed on the first call (SV caches built) and the second."""
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+    import gkmsvm_lite_b200.synthetic as syn
+
+    codes = syn.random_codes(np.random.default_rng(seed), n, L)
+    X = np.eye(4, dtype=np.float32)[codes].transpose(0, 2, 1).copy()
+    t0 = time.perf_counter()
+    base = gk.load_lsgkm_model(ENCODE_MODEL)
+    load_s = time.perf_counter() - t0
+    # a small model warms the library and the allocator, as the reference's
+    # benchmark warms its kernels
+    gk.GkmSVM(base.support_sequences[:600], base.coefficients[:600], base.bias, "gkm_esttrunc",
+              base.kernel_params).cuda()(X[:32]).cpu()
+    out = {"workload": f"72,145-SV ENCODE model (ENCFF579AOX, l=11 k=7 d=3), {n} synthetic {L} bp one-hot queries",
+           "model_load_s": load_s, "published_seqs_per_sec": ENCODE_PUBLISHED}
+    for name, kt, extra in (("t2", "gkm_esttrunc", {}), ("t3", "gkmrbf", {"gamma": 1.0})):
+        m = gk.GkmSVM(base.support_sequences, base.coefficients, base.bias, kt, {**base.kernel_params, **extra},
+                      sv_lengths=base.sv_lengths).cuda()
+        times = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            m(X).cpu()
+            times.append(time.perf_counter() - t0)
+        path = "l-mer table" if m._lmer_table is not None and m._lmer_table is not False else "l-mer index"
+        out[name] = {"first_s": times[0], "steady_s": min(times[1:]), "seqs_per_sec": n / min(times[1:]),
+                     "path": path, "vs_L40S": n / min(times[1:]) / ENCODE_PUBLISHED[name]["L40S"]}
+        del m
+    return out
+
+
+def masked_join_hits(sv_windows: int, l: int, j: int, n_masks: int, q: float = 0.2564) -> float:
+    """Expected exact-match hits per query window of the reference's masked
+    join (kernels/masked.py:45-69, 265-310) with n_masks masks keeping j of l
+    positions, over sv_windows indexed windows of i.i.d. bases with per-position
+    match probability q (GC 0.42: 0.29^2 * 2 + 0.21^2 * 2)."""
+    return n_masks * sv_windows * q**j
+
+
+def pairwise_forms_leg(n_small=4000, rows=64, seed=12):
+    """The shapes where the reference would take its masked join: t=0 gkm_cnt
+    l=11 k=7 with no d (dmax 4, 31,714 neighbour masks).  At the 72k-SV config-3
+    model the index applies (11.7 indexed windows per l-mer lift its limit to
+    32,768 neighbours, as the reference's kernels/lmer_index.py:97-109); with
+    n_small SVs of 300 bp it does not, and the autotuned all-pairs form (the
+    tensor-core product or the warp join) scores every window pair.  Beside
+    each: the masked join's own work, 330 masks of 7 kept positions (its plan
+    for h(m) = C(l - m, 7) is the single level j = 7)."""
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+    import gkmsvm_lite_b200.synthetic as syn
+    from gkmsvm_lite_b200 import engine
+    from math import comb
+
+    params = {"L": 11, "k": 7}
+    out = {"kernel": "t=0 gkm_cnt l=11 k=7 (no d: dmax 4, 31,714 neighbours)"}
+    sv, svl, coef = syn.config3_model()
+    xq, xl, _ = syn.config3_queries(n=2000)
+    rowsel = np.arange(rows)
+    L = int(xl[rowsel].max())
+    cases = [("config3_72k", sv, svl, coef)]
+    rng = np.random.default_rng(seed)
+    small = syn.random_codes(rng, n_small, 300)
+    cases.append((f"{n_small}_svs_300bp", small, None, rng.normal(0, 0.1, n_small)))
+    for name, s_codes, s_len, s_coef in cases:
+        m = gk.GkmSVM(s_codes, s_coef, 0.0, "gkm_cnt", params, sv_lengths=s_len).cuda()
+        m.use_lmer_table = False
+        nwin = m._n_sv_windows()
+        path = "index" if m._index_applies() else "all-pairs (autotuned)"
+        m(xq[:8, :L], lengths=xl[:8])  # builds the SV caches, tunes the pairwise form
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        m(xq[rowsel, :L], lengths=xl[rowsel])
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        qwin = int(np.clip(xl[rowsel] - 10, 0, None).sum())
+        out[name] = {"path": path, "sv_windows": nwin, "query_windows": qwin, "ms": ms,
+                     "seqs_per_sec": rows / (ms / 1e3),
+                     "window_pairs_per_query_window": nwin,
+                     "masked_join_hits_per_query_window": masked_join_hits(nwin, 11, 7, comb(11, 7)),
+                     "pairwise_tuned": {str(k): v for k, v in engine.PAIRWISE_TUNED.items()}}
+        del m
+    return out
+
+
 def gram_leg(n=4000, forms=("index", "dense", "join")):
     """Config 2: the normalised symmetric Gram matrix of n sequences (lengths
     log-uniform in 100..1000 bp), t=4 wgkm l=11 k=7 d=3, through
@@ -736,6 +839,8 @@ def run_b200(args):
                 result["ism_explain"] = ism_explain_leg(sv, svl, coef)
                 result["deltasvm"] = deltasvm_leg(sv, svl, coef)
                 result["gram"] = gram_leg(args.gram_n)
+                result["encode"] = encode_leg()
+                result["pairwise_forms"] = pairwise_forms_leg()
                 result["training"] = training_leg(args.gram_n)
     if rank == 0:
         # the oracle re-scores rows of the timed batch (the longest, the most
@@ -784,6 +889,12 @@ def main():
         import gkmsvm_lite_b200.synthetic as syn
 
         print(json.dumps(serving_leg(*syn.config3_model())), flush=True)
+        return 0
+    if args.leg == "pairwise-forms":
+        print(json.dumps(pairwise_forms_leg()), flush=True)
+        return 0
+    if args.leg == "encode":
+        print(json.dumps(encode_leg()), flush=True)
         return 0
     if args.leg == "explain-pairs":
         print(json.dumps(explain_pairs_leg()), flush=True)

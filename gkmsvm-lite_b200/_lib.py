@@ -52,10 +52,12 @@ COLUMNS_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int32, ctypes.POINTER(ctype
 SIGNATURES = {
     "gkm_version": [],
     "gkm_device_info": [P, P],
+    "gkm_set_thread_grid_limit": [I32],
     "gkm_pack": [SPEC, P, P, I64, I64, P, P, P, P],
     "gkm_self_kernel": [SPEC, P, P, P, I64, I64, P, P, P],
     "gkm_join_pairwise": [SPEC, P, P, I64, I64, P, P, P, I64, I64, P, P, P],
     "gkm_dense_pairwise": [SPEC, P, P, I64, I64, P, P, P, I64, I64, P, P, P, P],
+    "gkm_dense_set_role_wait": [I64],
     "gkm_index_create": [SPEC, P, P, P, I64, I64, P, I32, I32, P, P],
     "gkm_index_free": [P],
     "gkm_index_info": [P, P, P, P, P],
@@ -70,7 +72,8 @@ SIGNATURES = {
     "gkm_table_score": [SPEC, P, P, P, P, I64, I64, D, I32, P, P, P, P],
     "gkm_mutant_diag": [SPEC, P, P, I64, I64, I64, P, P, P],
     "gkm_ism_table": [SPEC, P, P, P, I64, I64, I64, P, P, P, I32, P, P],
-    "gkm_index_mutants": [P, P, P, I64, I64, I64, P, P, P, P, P, P, D, I32, P, P],
+    "gkm_index_mutants_workspace": [P, I64, I64, P, P],
+    "gkm_index_mutants": [P, P, P, I64, I64, I64, P, P, P, P, P, P, D, I32, P, P, I64, P],
     "gkm_raw_score": [P, I64, I64, P, P, P, D, I32, D, P, P],
     "gkm_impact": [P, I64, I64, P, P, P, D, I32, P, P],
     "gkm_explain_lmer": [SPEC, P, P, I64, I64, I64, P, P, P, P, P, I32, P, P, I32, P, P],

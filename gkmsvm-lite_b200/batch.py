@@ -246,3 +246,131 @@ class DirectScorer:
         if self.index is not None and self._rerun is not None:
             return self.index.settle(self._before, self._rerun)
         return False
+
+
+class _PerRowGraph:
+    """One bucket of a per-row pipeline (ISM, GkmExplain): fixed device
+    buffers codes [rows, L] and lengths [rows] (rows past the batch get length
+    0: no windows, no work) and one CUDA graph of the whole pass, captured on
+    the first call after an eager warm-up."""
+
+    def __init__(self, runner, rows: int, L: int):
+        dev = runner.model._device
+        self.rows, self.L = rows, L
+        self.codes = torch.zeros((rows, L), dtype=torch.uint8, device=dev)
+        self.lengths = torch.zeros(rows, dtype=torch.int64, device=dev)
+        self.out = None
+        self.graph = None
+        self._runner = weakref.ref(runner)
+
+    def _body(self):
+        self.out = self._runner().body(self.codes, self.lengths)
+
+    def run(self):
+        if self.graph is None:
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                self._body()  # warm-up: builds SV caches, tunes pairwise forms
+            torch.cuda.current_stream().wait_stream(side)
+            enabled = gc.isenabled()
+            gc.disable()
+            try:
+                self.graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(self.graph, capture_error_mode="thread_local"):
+                    self._body()
+            finally:
+                if enabled:
+                    gc.enable()
+        self.graph.replay()
+
+
+class _PerRowRunner:
+    """Shape-bucketed, graph-captured runs of a per-row pipeline: rows rounded
+    up to a multiple of row_granule, length to a power of two >= 64, so a few
+    graphs serve batches of uneven length; each replay is one launch of the
+    whole pass (packing, self-kernels, the persistent index queries over the
+    device work queue, the reductions).  Results equal the eager pass's."""
+
+    row_granule = 8
+
+    def __init__(self, model):
+        self.model = model
+        self._graphs: dict = {}
+
+    def body(self, codes, lengths):  # [rows, 4, L] on the device, no host synchronisation
+        raise NotImplementedError
+
+    def __call__(self, codes: torch.Tensor, lengths: torch.Tensor | None = None) -> torch.Tensor:
+        """[B, 4, L] of device codes [B, L] (lengths: device [B], None: all L);
+        0 past each row's length, rows shorter than l all 0 (the caller
+        marks them NaN)."""
+        B, L = codes.shape
+        key = (-(-B // self.row_granule) * self.row_granule, _bucket_len(max(L, self.model.kernel.l)))
+        g = self._graphs.get(key)
+        if g is None:
+            g = self._graphs[key] = _PerRowGraph(self, *key)
+        index = self.model._sv_index() if self.model.use_lmer_index else None
+        before = index.counters() if index is not None else None
+        g.codes[:B, :L].copy_(codes)
+        g.codes[:B, L:].zero_()
+        if lengths is None:
+            g.lengths[:B].fill_(L)
+        else:
+            g.lengths[:B].copy_(lengths)
+        g.lengths[B:].zero_()
+        g.run()
+        if index is not None:
+            # 16-bit counter carries that outgrew a block's log: rerun exactly
+            index.settle(before, g._body)
+        out = g.out[:B, :, :L]
+        past = torch.arange(L, device=out.device)[None, None, :] >= g.lengths[:B, None, None]
+        return out.masked_fill(past, 0.0)
+
+
+class BatchedIsm(_PerRowRunner):
+    """gkmsvm_lite_b200.ism of device code batches through bucket graphs."""
+
+    def __init__(self, model):
+        super().__init__(model)
+        self._work = None
+        self._works = []  # every workspace a captured graph refers to
+
+    def body(self, codes, lengths):
+        from . import ism as _ism
+
+        m = self.model
+        work = None
+        if m._lmer_table_for() is None:
+            # the index path's workspace, shared by the buckets (their replays
+            # are serial); grown for a bucket of more rows (the eager warm-up
+            # allocates it, never the capture)
+            need = _ism.ism_workspace_bytes(m, codes.shape[0], codes.shape[1])
+            if self._work is None or self._work.numel() < need:
+                self._work = torch.empty(need, dtype=torch.uint8, device=codes.device)
+                self._works.append(self._work)
+            work = self._work
+        return _ism._ism_rows(m, codes, lengths, codes.device, check=False, work=work)
+
+
+class BatchedExplain(_PerRowRunner):
+    """gkmsvm_lite_b200.gkmexplain of device code batches through bucket
+    graphs, for one mode ("importance", "hypothetical" or "perturbation")."""
+
+    def __init__(self, model, mode: str = "hypothetical"):
+        super().__init__(model)
+        from .explain import _MODE_ALIASES
+
+        self.mode = _MODE_ALIASES[mode]
+        self._table = {}
+
+    def body(self, codes, lengths):
+        from . import explain as _ex
+
+        m = self.model
+        pert = self.mode == "perturbation"
+        if pert not in self._table:
+            # the explain table, if the model's switch calls for one, is chosen
+            # once per runner (a large call's cost model)
+            self._table[pert] = _ex._explain_table(m, 1 << 62, pert, codes.device)
+        return _ex._explain_rows(m, codes, lengths, self.mode, codes.device, self._table[pert], check=False)

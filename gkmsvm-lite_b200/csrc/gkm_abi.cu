@@ -16,6 +16,25 @@ int gkm_fail(int code, const char *fmt, ...)
     return code;
 }
 
+// Persistent index queries launched from a thread take at most this many
+// blocks (0: one per SM).  A serving loop's side worker (ISM, GkmExplain) sets
+// it so that its long queries leave SMs free for the scoring passes of other
+// threads; nothing is shared between threads.
+static thread_local int32_t g_grid_limit = 0;
+
+extern "C" int gkm_set_thread_grid_limit(int32_t blocks)
+{
+    if (blocks < 0) return gkm_fail(GKM_ERR_INVALID, "grid limit %d < 0", blocks);
+    g_grid_limit = blocks;
+    return GKM_OK;
+}
+
+int gkm_query_blocks()
+{
+    const int n = gkm_sm_count();
+    return g_grid_limit > 0 && g_grid_limit < n ? g_grid_limit : n;
+}
+
 int gkm_cuda_status(cudaError_t e, const char *what)
 {
     if (e == cudaSuccess) return GKM_OK;

@@ -135,3 +135,6 @@ struct gkm_index {
 
 int gkm_smem_limit();
 int gkm_sm_count();
+// Blocks a persistent index query may take on the calling thread's launches:
+// the SM count, or the thread's limit (gkm_set_thread_grid_limit) if lower.
+int gkm_query_blocks();

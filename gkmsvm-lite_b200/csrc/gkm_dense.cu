@@ -180,15 +180,18 @@ __device__ __forceinline__ bool bar_test(uint32_t bar, uint32_t parity)
 }
 
 // Waits for the phase of `bar` with parity `parity` to complete.  False when
-// another role has aborted (*abort set) or after D_WAIT_NS, which sets *abort
-// and the launch's error flag.
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, volatile int *abort, int *error)
+// another role has aborted (*abort set) or after limit_ns, which sets *abort
+// and the launch's error flag.  Hand-offs between roles wait up to the
+// launch's role limit (D_WAIT_NS unless a test shortens it); the drain waits
+// for copies and MMAs in flight always wait up to D_WAIT_NS.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, volatile int *abort, int *error,
+                                         uint64_t limit_ns = D_WAIT_NS)
 {
     const uint64_t t0 = global_ns();
     for (;;) {
         if (bar_test(bar, parity)) return true;
         if (*abort) return false;
-        if (global_ns() - t0 > D_WAIT_NS) {
+        if (global_ns() - t0 > limit_ns) {
             *abort = 1;
             atomicOr(error, 1);
             return false;
@@ -230,6 +233,7 @@ struct DenseArgs {
     double *raw;
     uint64_t *profile;
     int *error;
+    uint64_t role_wait_ns;  // limit of the hand-off waits between roles
 };
 
 // chunk-local windows of SV chunk `cg`: prefix counts pre[0..n] (n SVs)
@@ -378,12 +382,14 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
                 // wait for this B tile to land even when none of its tiles is
                 // ours: the release below must not count toward an earlier
                 // phase of the buffer while the other warpgroup still reads it
-                bool ok = __all_sync(GKM_FULL, bar_wait(bar(BAR_BFULL + buf), (g / D_BBUF) & 1u, abort, a.error));
+                bool ok = __all_sync(GKM_FULL, bar_wait(bar(BAR_BFULL + buf), (g / D_BBUF) & 1u, abort, a.error,
+                                                                   a.role_wait_ns));
                 if (!ok) break;
                 for (int at = 0; at < NA; at++) {
                     const uint32_t t = t_base + (uint32_t)(bt * NA + at), slot = t & 1u;
                     if (slot != eg) continue;
-                    ok = __all_sync(GKM_FULL, bar_wait(bar(BAR_TFULL + slot), (t >> 1) & 1u, abort, a.error));
+                    ok = __all_sync(GKM_FULL, bar_wait(bar(BAR_TFULL + slot), (t >> 1) & 1u, abort, a.error,
+                                                                  a.role_wait_ns));
                     if (!ok) break;
                     asm volatile("tcgen05.fence::after_thread_sync;");
                     // the whole accumulator row in 64 registers (values < 48), then
@@ -457,7 +463,9 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
             if (lane == 0) {
                 for (int bt = 0; bt < NB; bt++) {
                     const uint32_t g = g_base + bt, buf = g % D_BBUF;
-                    if (g >= D_BBUF && !bar_wait(bar(BAR_BEMPTY + buf), (g / D_BBUF - 1) & 1u, abort, a.error)) break;
+                    if (g >= D_BBUF &&
+                        !bar_wait(bar(BAR_BEMPTY + buf), (g / D_BBUF - 1) & 1u, abort, a.error, a.role_wait_ns))
+                        break;
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar(BAR_BFULL + buf)),
                                  "r"((uint32_t)REC)
                                  : "memory");
@@ -474,10 +482,10 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
             bool ok = true;
             for (int bt = 0; bt < NB && ok; bt++) {
                 const uint32_t g = g_base + bt, buf = g % D_BBUF;
-                ok = bar_wait(bar(BAR_BFULL + buf), (g / D_BBUF) & 1u, abort, a.error);
+                ok = bar_wait(bar(BAR_BFULL + buf), (g / D_BBUF) & 1u, abort, a.error, a.role_wait_ns);
                 for (int at = 0; at < NA && ok; at++) {
                     const uint32_t t = t_base + (uint32_t)(bt * NA + at), slot = t & 1u;
-                    if (t >= 2) ok = bar_wait(bar(BAR_TEMPTY + slot), ((t >> 1) - 1) & 1u, abort, a.error);
+                    if (t >= 2) ok = bar_wait(bar(BAR_TEMPTY + slot), ((t >> 1) - 1) & 1u, abort, a.error, a.role_wait_ns);
                     if (!ok) break;
                     asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
@@ -533,7 +541,18 @@ __global__ void __launch_bounds__(D_THREADS, 2) dense_pairs_kernel(DenseArgs a)
     }
 }
 
+// Role hand-off wait limit of the dense launches made from this thread; 0:
+// D_WAIT_NS.  Tests shorten it to make a hand-off wait run out.
+static thread_local uint64_t g_role_wait_ns = 0;
+
 }  // namespace
+
+extern "C" int gkm_dense_set_role_wait(int64_t ns)
+{
+    if (ns < 0) return gkm_fail(GKM_ERR_INVALID, "wait limit %lld < 0", (long long)ns);
+    g_role_wait_ns = (uint64_t)ns;
+    return GKM_OK;
+}
 
 extern "C" int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, const int32_t *cx, int64_t B,
                                   int64_t Wx, const uint32_t *by, const uint32_t *ry, const int32_t *cy, int64_t S,
@@ -578,6 +597,7 @@ extern "C" int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, cons
     a.raw = raw;
     a.profile = profile;
     a.error = error;
+    a.role_wait_ns = g_role_wait_ns ? g_role_wait_ns : D_WAIT_NS;
     cudaFuncSetAttribute(dense_pairs_kernel<MODE_U32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          Cfg<MODE_U32>::SMEM);
     cudaFuncSetAttribute(dense_pairs_kernel<MODE_U64>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -377,6 +377,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
     extern __shared__ __align__(16) uint8_t smraw[];
     __shared__ double red[32];
     __shared__ int nlog;
+    __shared__ unsigned long long chk[2];  // decoded field sum, plain adds made
     const int n_masks = a.n_masks;
     uint32_t *sm_masks = n_masks <= MASKS_SMEM_MAX ? (uint32_t *)smraw : nullptr;
     uint32_t *sm_log = (uint32_t *)(smraw + ((sm_masks ? (size_t)n_masks * 4 : 0) + 15 & ~(size_t)15));
@@ -420,80 +421,150 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         const int sub_n = min(sub, ns - sub_lo);
         const int stride = C16 ? St : sub_n;
         const int nacc = C16 ? ((a.nlev + 1) / 2) * St : a.nlev * sub_n;
-        for (int k = threadIdx.x; k < nacc; k += Q_THREADS) sm_acc[k] = 0;
-        if (threadIdx.x == 0) nlog = 0;
-        __syncthreads();
         const uint32_t id_lo = max((uint32_t)sub_lo, lo), id_hi = (uint32_t)(sub_lo + sub_n);
-        // work units (window, mask group): rows of fewer windows than warps
-        // share each window's masks among g warps, so every warp has work
+        // 16-bit counters: a first attempt with plain shared adds (no return
+        // value, no per-hit carry test), checked exactly at the end -- the
+        // decoded fields sum to the hits counted unless some field carried;
+        // only then the item is redone with the carry-logged adds
+        bool logged = false;
+        for (;;) {
+        for (int k = threadIdx.x; k < nacc; k += Q_THREADS) sm_acc[k] = 0;
+        if (threadIdx.x == 0) {
+            nlog = 0;
+            chk[0] = chk[1] = 0;
+        }
+        __syncthreads();
+        uint32_t lane_hits = 0;  // per lane (<= its rounds x 1): plain adds made
+        // work units (window, chunk of 32 masks), window-major, split evenly
+        // into one contiguous range per warp: short rows (ISM window sets,
+        // row splits) keep every warp busy, long rows leave no idle last round
         const int nwin = i1 - i0;
-        const int g = nwin >= Q_WARPS ? 1 : max(1, min(Q_WARPS / max(nwin, 1), (n_masks + 31) / 32));
-        for (int wu = warp; wu < nwin * g; wu += Q_WARPS) {
-            const int i = i0 + wu / g, kg = wu - (wu / g) * g;
-            const uint32_t u = x[i];
-            const uint32_t wq = WEIGHTED ? (a.wq ? (uint32_t)a.wq[row * a.W + i] : gkm_wt(a.wd, n, i)) : 1u;
-            // per lane: its mask's bucket and counter slot (C16: word base and
-            // field of the level; wide: row base of the level)
-            uint32_t beg = 0, end = 0, base = 0, add = 0, fmask = 0;
-            auto lane_mask = [&](int c, uint32_t &b0, uint32_t &e0, uint32_t &bs, uint32_t &ad, uint32_t &fm) {
-                const uint32_t mk = masks[c];
-                const uint32_t v = u ^ (mk & 0x00FFFFFFu);
-                const uint32_t lev = mk >> 24;
-                if (C16) {
-                    bs = (lev >> 1) * (uint32_t)St;
-                    ad = 1u << (16 * (lev & 1u));
-                    fm = 0xFFFFu << (16 * (lev & 1u));
-                } else {
-                    bs = lev * (uint32_t)stride - (uint32_t)sub_lo;
+        const int nchunk = (n_masks + 31) >> 5;
+        const int64_t nunit = (int64_t)nwin * nchunk;
+        const int64_t ub = nunit * warp / Q_WARPS, ue = nunit * (warp + 1) / Q_WARPS;
+        // per lane: its mask's bucket (begin, length) and counter slot (C16:
+        // word base of the level pair | the level's half in bit 31; wide: row
+        // base of the level)
+        auto lane_mask = [&](uint32_t u, int c, uint32_t &b0, uint32_t &n0, uint32_t &sl) {
+            b0 = n0 = sl = 0;
+            if (c >= n_masks) return;
+            const uint32_t mk = masks[c];
+            const uint32_t v = u ^ (mk & 0x00FFFFFFu);
+            const uint32_t lev = mk >> 24;
+            sl = C16 ? ((lev >> 1) * (uint32_t)St) | ((lev & 1u) << 31) : lev * (uint32_t)stride - (uint32_t)sub_lo;
+            // the bucket's bounds from the aligned group of four offsets
+            // holding off[v] (a second load only when off[v + 1] starts the
+            // next group)
+            const uint4 q = __ldg((const uint4 *)(off + (v & ~3u)));
+            const uint32_t r = v & 3u;
+            b0 = r == 0 ? q.x : r == 1 ? q.y : r == 2 ? q.z : q.w;
+            const uint32_t e0 = r == 0 ? q.y : r == 1 ? q.z : r == 2 ? q.w : __ldg(off + v + 1);
+            n0 = e0 - b0;
+        };
+        auto window_weight = [&](int i) -> uint32_t {
+            return WEIGHTED ? (a.wq ? (uint32_t)a.wq[row * a.W + i] : gkm_wt(a.wd, n, i)) : 1u;
+        };
+        if (ub < ue) {
+            int win = (int)(ub / nchunk), ch = (int)(ub - (int64_t)win * nchunk);
+            uint32_t u = x[i0 + win], wq = window_weight(i0 + win);
+            uint32_t beg, len, slot;
+            lane_mask(u, ch * 32 + lane, beg, len, slot);
+            for (int64_t un = ub; un < ue; un++) {
+                // the next unit's window and buckets, loaded while this one is counted
+                int nw = win, nc = ch + 1;
+                if (nc == nchunk) {
+                    nw = win + 1;
+                    nc = 0;
                 }
-                b0 = __ldg(off + v);
-                e0 = __ldg(off + v + 1);
-            };
-            if (kg * 32 + lane < n_masks) lane_mask(kg * 32 + lane, beg, end, base, add, fmask);
-            for (int c0 = kg * 32; c0 < n_masks; c0 += 32 * g) {
-                uint32_t nbeg = 0, nend = 0, nbase = 0, nadd = 0, nfm = 0;
-                const int cn = c0 + 32 * g + lane;
-                if (cn < n_masks) lane_mask(cn, nbeg, nend, nbase, nadd, nfm);
-                // the bucket in aligned blocks of four entries, one vector load each
-                for (uint32_t e = beg & ~3u; __any_sync(GKM_FULL, e < end); e += 4) {
-                    uint32_t en[4];
-                    if (e < end) {
-                        if (E16) {
-                            const uint2 w = __ldg((const uint2 *)((const uint16_t *)a.ent + e));
-                            en[0] = w.x & 0xFFFFu;
-                            en[1] = w.x >> 16;
-                            en[2] = w.y & 0xFFFFu;
-                            en[3] = w.y >> 16;
-                        } else {
-                            const uint4 w = __ldg((const uint4 *)((const uint32_t *)a.ent + e));
-                            en[0] = w.x;
-                            en[1] = w.y;
-                            en[2] = w.z;
-                            en[3] = w.w;
-                        }
+                uint32_t nu = u, nwq = wq, nbeg = 0, nlen = 0, nslot = 0;
+                if (un + 1 < ue) {
+                    if (nw != win) {
+                        nu = x[i0 + nw];
+                        nwq = window_weight(i0 + nw);
                     }
+                    lane_mask(nu, nc * 32 + lane, nbeg, nlen, nslot);
+                }
+                // the warp's 32 buckets as one list of entries: bucket i holds
+                // list positions [excl_i, excl_i + len_i); a round gives lane j
+                // position f0 + j
+                uint32_t incl = len;
 #pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        if (e + q < beg || e + q >= end) continue;
-                        const uint32_t id = E16 ? en[q] : (en[q] & 0x00FFFFFFu);
-                        if (RANGE && (id < id_lo || id >= id_hi)) continue;
-                        if (C16)
-                            count16(sm_acc, base + id, add, fmask, &nlog, sm_log, a.status);
-                        else {
-                            const uint32_t inc = WEIGHTED ? wq * (en[q] >> 24) : 1u;
-                            const uint32_t old = atomicAdd(sm_acc + base + id, inc);
-                            if (old + inc < old) atomicAdd(a.status + 1, 1u);
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(GKM_FULL, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const uint32_t total = __shfl_sync(GKM_FULL, incl, 31);
+                const uint32_t excl = incl - len;
+                const uint32_t dbase = beg - excl;  // entry index = dbase_i + list position
+                // lor: lane r holds the lane of the r-th non-empty bucket
+                const uint32_t nz = __ballot_sync(GKM_FULL, len != 0);
+                uint32_t lor = 0;
+#pragma unroll
+                for (int s = 16; s; s >>= 1)
+                    if (__popc(nz & ((1u << (lor + s)) - 1u)) <= (uint32_t)lane) lor += s;
+                uint32_t started = 0;  // non-empty buckets that began in earlier rounds
+                for (uint32_t f0 = 0; f0 < total; f0 += 32) {
+                    // non-empty buckets beginning in this round, by position
+                    const uint32_t p = excl - f0;
+                    const uint32_t starts = __reduce_or_sync(GKM_FULL, (len != 0 && p < 32u) ? 1u << p : 0u);
+                    const uint32_t rank = started + __popc(starts & (0xFFFFFFFFu >> (31 - lane))) - 1u;
+                    started += __popc(starts);
+                    const int src = __shfl_sync(GKM_FULL, (int)lor, (int)(rank & 31u));
+                    const uint32_t eb = __shfl_sync(GKM_FULL, dbase, src);
+                    const uint32_t sl = __shfl_sync(GKM_FULL, slot, src);
+                    const uint32_t f = f0 + lane;
+                    if (f >= total) continue;
+                    const uint32_t en = load_entry<E16>(a.ent, eb + f);
+                    const uint32_t id = E16 ? en : (en & 0x00FFFFFFu);
+                    if (RANGE && (id < id_lo || id >= id_hi)) continue;
+                    if (C16) {
+                        const uint32_t sh = (sl >> 31) * 16u;
+                        if (logged) {
+                            count16(sm_acc, (sl & 0x7FFFFFFFu) + id, 1u << sh, 0xFFFFu << sh, &nlog, sm_log,
+                                    a.status);
+                        } else {
+                            atomicAdd(sm_acc + (sl & 0x7FFFFFFFu) + id, 1u << sh);
+                            lane_hits++;
                         }
+                    } else {
+                        const uint32_t inc = WEIGHTED ? wq * (en >> 24) : 1u;
+                        const uint32_t old = atomicAdd(sm_acc + sl + id, inc);
+                        if (old + inc < old) atomicAdd(a.status + 1, 1u);
                     }
                 }
                 beg = nbeg;
-                end = nend;
-                base = nbase;
-                add = nadd;
-                fmask = nfm;
+                len = nlen;
+                slot = nslot;
+                win = nw;
+                ch = nc;
+                u = nu;
+                wq = nwq;
             }
         }
         __syncthreads();
+        if (!C16 || logged) break;
+        {
+            unsigned long long fs = 0, hs = lane_hits;
+            for (int k = threadIdx.x; k < nacc; k += Q_THREADS) {
+                const uint32_t v = sm_acc[k];
+                fs += (v & 0xFFFFu) + (v >> 16);
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                fs += __shfl_xor_sync(GKM_FULL, fs, o);
+                hs += __shfl_xor_sync(GKM_FULL, hs, o);
+            }
+            if (lane == 0) {
+                atomicAdd(&chk[0], fs);
+                atomicAdd(&chk[1], hs);
+            }
+        }
+        __syncthreads();
+        const bool exact = chk[0] == chk[1];
+        __syncthreads();  // every thread has read chk before the retry resets it
+        if (exact) break;
+        logged = true;
+        }
         const int nl = min(nlog, LOG_CAP);
         if (MODE == MODE_COUNT) {
             for (int s = sub_lo + threadIdx.x; s < sub_lo + sub_n; s += Q_THREADS) {
@@ -790,7 +861,8 @@ static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cu
     cudaError_t e0 = cudaMemsetAsync(q.queue, 0, sizeof(unsigned int), st);
     if (e0 != cudaSuccess) return gkm_cuda_status(e0, "index queue");
     int64_t items = B * ix->tiles * a.nsplit;
-    unsigned grid = (unsigned)(items < gkm_sm_count() ? items : gkm_sm_count());
+    const int blocks = gkm_query_blocks();
+    unsigned grid = (unsigned)(items < blocks ? items : blocks);
     if (ix->spec.weighted)
         launch_query<true, MODE, false, false>(grid, smem, st, q);
     else if (ix->ent16 && ix->wide)
@@ -811,7 +883,7 @@ static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cu
 // kept within 256 MB.  1: no split.
 static int split_plan(const gkm_index_t *ix, int64_t B, int64_t W)
 {
-    const int64_t items = B * ix->tiles, target = 2LL * gkm_sm_count();
+    const int64_t items = B * ix->tiles, target = 2LL * gkm_query_blocks();
     if (items >= target || W < 64) return 1;
     if (B * ix->S * ix->nlev * 8 > (256LL << 20)) return 1;
     int64_t ns = (target + items - 1) / items;
@@ -1027,11 +1099,16 @@ extern "C" int gkm_index_count(const gkm_index_t *ix, const uint32_t *bx, const 
 }
 
 // ---------------------------------------------------------------------------
-// ISM through the index (kernels/lmer_index_cpu.py:203-285): per (position p,
-// row b), the windows covering p before (set 0) and after each of the three
-// substitutions (sets 1..3) are queried as rows of <= l windows that keep their
-// slot weights (ism.py:276-295); then K(mutant, s) = ref[b, s] + K(set v, s) -
-// K(set 0, s), and the reference base's own delta is exactly 0.
+// ISM through the index (kernels/lmer_index_cpu.py:203-285): K(mutant, s) =
+// ref[b, s] + K(mutated windows, s) - K(reference windows, s), over the <= l
+// windows covering the mutated base p (they keep their slot weights,
+// ism.py:276-295).  Per chunk of positions, one query covers
+//   * the three mutant window sets of each (p, b), one query row each (the
+//     reference base's own set is the reference and its delta exactly 0), and
+//   * every reference window the chunk's positions touch, once, as a row of
+//     its own: a position's reference-window term is the sum of the rows of
+//     the windows covering it (each window covers l positions, so querying it
+//     once instead of once per covered position drops (l - 1) / l of that part).
 // ---------------------------------------------------------------------------
 
 // the base at p as packed in the first window covering it (-1: none covers p)
@@ -1040,135 +1117,175 @@ __device__ __forceinline__ int ism_ref_base(const uint32_t *fwd, int64_t b, int6
     return a_e > a_s ? (int)((fwd[b * W + a_s] >> (2 * (p - a_s))) & 3u) : -1;
 }
 
-// sets per (position, row): 0 = the reference windows covering p; 1..3 = the
-// same windows with the three other bases at p, in increasing base order (the
-// reference base's own set would repeat set 0, and its delta is exactly 0)
-constexpr int ISM_SETS = 4;
+// rows of one chunk: 3 mutant sets per (position, row), then per row the
+// reference windows p0 - l + 1 .. p0 + np - 1; every query row has l slots
+struct IsmChunk {
+    int64_t np, B, nw0;  // positions, rows, reference windows per row (np + l - 1)
+    __host__ __device__ int64_t mut_rows() const { return 3 * np * B; }
+    __host__ __device__ int64_t rows() const { return mut_rows() + B * nw0; }
+};
 
-__global__ void ism_sets_kernel(gkm_spec spec, const uint32_t *__restrict__ fwd, const int32_t *__restrict__ cnt,
-                                int64_t B, int64_t W, int64_t p0, int64_t nitems, uint32_t *__restrict__ rows,
+__global__ void ism_rows_kernel(gkm_spec spec, const uint32_t *__restrict__ fwd, const int32_t *__restrict__ cnt,
+                                int64_t W, int64_t p0, IsmChunk ck, uint32_t *__restrict__ rows,
                                 int32_t *__restrict__ rcount, uint8_t *__restrict__ rwt)
 {
-    int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (it >= nitems) return;
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= ck.rows()) return;
     const int l = spec.l;
-    int64_t p = p0 + it / B, b = it % B;
-    int n = cnt[b];
-    int a_s = (int)(p - l + 1 > 0 ? p - l + 1 : 0);
-    int a_e = (int)(p + 1 < n ? p + 1 : n);
-    int na = a_e > a_s ? a_e - a_s : 0;
-    const int xp = ism_ref_base(fwd, b, W, p, a_s, a_e);
-    for (int r = 0; r < ISM_SETS; r++) {
-        int64_t row = it * ISM_SETS + r;
-        const int v = r == 0 ? -1 : (r - 1) + ((r - 1) >= xp ? 1 : 0);
-        rcount[row] = na;
-        for (int j = 0; j < l; j++) {
-            uint32_t w = GKM_PAD;
-            uint8_t wt = 0;
-            if (j < na) {
-                int i = a_s + j;
-                w = fwd[b * W + i];
-                if (r > 0) {
-                    uint32_t sh = 2u * (uint32_t)(p - i);
-                    w = (w & ~(3u << sh)) | ((uint32_t)v << sh);
-                }
-                wt = spec.weighted ? (uint8_t)gkm_wt(spec.wd, n, i) : 1;
-            }
-            rows[row * l + j] = w;
-            if (rwt) rwt[row * l + j] = wt;
+    uint32_t *row = rows + r * l;
+    uint8_t *wt = rwt ? rwt + r * l : nullptr;
+    for (int j = 0; j < l; j++) {
+        row[j] = GKM_PAD;
+        if (wt) wt[j] = 0;
+    }
+    if (r < ck.mut_rows()) {
+        const int64_t item = r / 3, p = p0 + item / ck.B, b = item % ck.B;
+        const int n = cnt[b];
+        const int a_s = (int)(p - l + 1 > 0 ? p - l + 1 : 0), a_e = (int)(p + 1 < n ? p + 1 : n);
+        const int na = a_e > a_s ? a_e - a_s : 0;
+        const int xp = ism_ref_base(fwd, b, W, p, a_s, a_e);
+        const int k = (int)(r - item * 3);       // the k-th base other than xp
+        const int v = k + (k >= xp ? 1 : 0);
+        rcount[r] = na;
+        for (int j = 0; j < na; j++) {
+            const int i = a_s + j;
+            const uint32_t sh = 2u * (uint32_t)(p - i);
+            row[j] = (fwd[b * W + i] & ~(3u << sh)) | ((uint32_t)v << sh);
+            if (wt) wt[j] = (uint8_t)gkm_wt(spec.wd, n, i);
+        }
+    } else {
+        const int64_t k = r - ck.mut_rows(), b = k / ck.nw0;
+        const int64_t i = p0 - l + 1 + (k - b * ck.nw0);
+        const bool in = i >= 0 && i < cnt[b];
+        rcount[r] = in ? 1 : 0;
+        if (in) {
+            row[0] = fwd[b * W + i];
+            if (wt) wt[0] = (uint8_t)gkm_wt(spec.wd, cnt[b], (int)i);
         }
     }
 }
 
-__global__ void ism_index_finish(const double *__restrict__ kset, int64_t S, const uint32_t *__restrict__ fwd,
-                                 const int32_t *__restrict__ cnt, int64_t B, int64_t W, int64_t L, int l,
-                                 int64_t p0, const double *__restrict__ ref, const double *__restrict__ ref_score,
-                                 const double *__restrict__ inv_dx, const double *__restrict__ inv_dmut,
-                                 const double *__restrict__ inv_ds, const double *__restrict__ coef,
-                                 double gamma, int rbf, double *__restrict__ out)
+// one block per (position, row) of the chunk: the three mutants' scores minus
+// the reference score; the reference base's own delta is exactly 0
+__global__ void ism_index_finish(const double *__restrict__ kbuf, int64_t S, const uint32_t *__restrict__ fwd,
+                                 const int32_t *__restrict__ cnt, int64_t W, int64_t L, int l, int64_t p0,
+                                 IsmChunk ck, const double *__restrict__ ref, const double *__restrict__ ref_score,
+                                 const double *__restrict__ inv_dmut, const double *__restrict__ inv_ds,
+                                 const double *__restrict__ coef, double gamma, int rbf, double *__restrict__ out)
 {
     __shared__ double red[32];
-    int64_t it = blockIdx.x;
-    int64_t p = p0 + it / B, b = it % B;
-    int n = cnt[b];
-    int a_s = (int)(p - l + 1 > 0 ? p - l + 1 : 0);
-    int a_e = (int)(p + 1 < n ? p + 1 : n);
+    const int64_t item = blockIdx.x, p = p0 + item / ck.B, b = item % ck.B;
+    const int n = cnt[b];
+    const int a_s = (int)(p - l + 1 > 0 ? p - l + 1 : 0), a_e = (int)(p + 1 < n ? p + 1 : n);
     const int xp = ism_ref_base(fwd, b, W, p, a_s, a_e);
-    const double *k0 = kset + (it * ISM_SETS) * S;
-    const double *rr = ref + b * S;
-    for (int v = 0; v < 4; v++) {
-        double z = inv_dmut[((int64_t)v * L + p) * B + b];
-        if (a_e <= a_s || v == xp) {  // the reference itself: exactly 0
-            if (threadIdx.x == 0) out[(b * 4 + v) * L + p] = 0.0;
-            continue;
-        }
-        const double *kv = kset + (it * ISM_SETS + 1 + v - (v > xp ? 1 : 0)) * S;
-        double acc = 0.0;
-        for (int64_t s = threadIdx.x; s < S; s += blockDim.x) {
-            double k = (rr[s] + (kv[s] - k0[s])) * z * inv_ds[s];
-            acc += coef[s] * (rbf ? exp(gamma * (k - 1.0)) : k);
-        }
-        acc = gkm_block_sum(acc, red);
-        if (threadIdx.x == 0) out[(b * 4 + v) * L + p] = acc - ref_score[b];
+    if (a_e <= a_s) {  // no window covers p
+        if (threadIdx.x < 4) out[(b * 4 + threadIdx.x) * L + p] = 0.0;
+        return;
     }
+    // rows of the reference windows a_s .. a_e - 1 of row b
+    const double *kw = kbuf + (ck.mut_rows() + b * ck.nw0 + (a_s - (p0 - l + 1))) * S;
+    const double *km = kbuf + item * 3 * S;
+    const double *rr = ref + b * S;
+    double z[3];
+    for (int k = 0; k < 3; k++) {
+        const int v = k + (k >= xp ? 1 : 0);
+        z[k] = inv_dmut[((int64_t)v * L + p) * ck.B + b];
+    }
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int64_t s = threadIdx.x; s < S; s += blockDim.x) {
+        double k0 = 0.0;
+        for (int j = 0; j < a_e - a_s; j++) k0 += kw[j * S + s];
+        const double base = rr[s] - k0, ds = inv_ds[s], c = coef[s];
+        for (int k = 0; k < 3; k++) {
+            const double kn = (base + km[k * S + s]) * z[k] * ds;
+            acc[k] += c * (rbf ? exp(gamma * (kn - 1.0)) : kn);
+        }
+    }
+    for (int k = 0; k < 3; k++) {
+        const double t = gkm_block_sum(acc[k], red);
+        const int v = k + (k >= xp ? 1 : 0);
+        if (threadIdx.x == 0) out[(b * 4 + v) * L + p] = t - ref_score[b];
+    }
+    if (threadIdx.x == 0) out[(b * 4 + xp) * L + p] = 0.0;
+}
+
+static size_t ism_align(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// workspace bytes of a chunk: query rows (l slots), their counts and slot
+// weights, and their K_raw rows
+static size_t ism_chunk_bytes(const gkm_index_t *ix, const IsmChunk &ck)
+{
+    const size_t rows = (size_t)ck.rows(), l = (size_t)ix->spec.l;
+    return ism_align(rows * l * 4) + ism_align(rows * 4) + ism_align(rows * l) + rows * (size_t)ix->S * 8;
+}
+
+extern "C" int gkm_index_mutants_workspace(const gkm_index_t *ix, int64_t B, int64_t L, int64_t *min_bytes,
+                                           int64_t *all_bytes)
+{
+    if (!ix || B < 0 || L < 0) return gkm_fail(GKM_ERR_INVALID, "null index or negative size");
+    const int64_t l = ix->spec.l;
+    if (min_bytes) *min_bytes = (int64_t)ism_chunk_bytes(ix, IsmChunk{1, B, l});
+    if (all_bytes) *all_bytes = (int64_t)ism_chunk_bytes(ix, IsmChunk{L, B, L + l - 1});
+    return GKM_OK;
 }
 
 extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, const int32_t *counts, int64_t B,
                                  int64_t W, int64_t L, const double *ref_raw, const double *ref_score,
                                  const double *inv_dx, const double *inv_dmut, const double *inv_ds,
-                                 const double *coef, double gamma, int32_t rbf, double *out, gkm_stream_t stream)
+                                 const double *coef, double gamma, int32_t rbf, double *out, void *workspace,
+                                 int64_t workspace_bytes, gkm_stream_t stream)
 {
-    if (!ix || !fwd || !counts || !ref_raw || !ref_score || !inv_dx || !inv_dmut || !inv_ds || !coef || !out)
+    (void)inv_dx;
+    if (!ix || !fwd || !counts || !ref_raw || !ref_score || !inv_dmut || !inv_ds || !coef || !out)
         return gkm_fail(GKM_ERR_INVALID, "null argument");
+    if (B < 0 || L < 0 || W < 0) return gkm_fail(GKM_ERR_INVALID, "negative size");
     if (B == 0 || L == 0) return GKM_OK;
+    if (!workspace || ((uintptr_t)workspace & 255))
+        return gkm_fail(GKM_ERR_INVALID, "ISM workspace must be non-null and 256-byte aligned");
     cudaStream_t st = (cudaStream_t)stream;
     const int l = ix->spec.l;
     const int64_t S = ix->S;
-    int64_t per_item = ISM_SETS * S * (int64_t)sizeof(double);
-    int64_t chunk = (1LL << 30) / per_item;
-    if (chunk < 1) chunk = 1;
-    int64_t total = L * B;
-    if (chunk > total) chunk = total;
-    if (chunk > (1LL << 31) - 1) chunk = (1LL << 31) - 1;
-    chunk = (chunk / B) * B;  // whole positions per chunk
-    if (chunk < B) chunk = B;
-    uint32_t *rows = nullptr;
-    int32_t *rc = nullptr;
-    uint8_t *rw = nullptr;
-    double *kset = nullptr;
-    int s = GKM_OK;
-    if (cudaMallocAsync(&rows, sizeof(uint32_t) * chunk * ISM_SETS * l, st) != cudaSuccess ||
-        cudaMallocAsync(&rc, sizeof(int32_t) * chunk * ISM_SETS, st) != cudaSuccess ||
-        cudaMallocAsync(&rw, chunk * ISM_SETS * l, st) != cudaSuccess ||
-        cudaMallocAsync(&kset, sizeof(double) * chunk * ISM_SETS * S, st) != cudaSuccess)
-        s = gkm_fail(GKM_ERR_OOM, "ISM scratch");
-    for (int64_t p0 = 0; s == GKM_OK && p0 < L; p0 += chunk / B) {
-        int64_t np = chunk / B;
-        if (p0 + np > L) np = L - p0;
-        int64_t nitems = np * B;
-        GKM_PREFER_SHARED(ism_sets_kernel);
-        ism_sets_kernel<<<(unsigned)((nitems + 127) / 128), 128, 0, st>>>(ix->spec, fwd, counts, B, W, p0, nitems,
-                                                                           rows, rc, rw);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) {
-            s = gkm_cuda_status(e, "ism_sets");
-            break;
+    // the most positions per chunk the workspace holds
+    int64_t np = 0;
+    for (int64_t lo = 1, hi = L; lo <= hi;) {
+        const int64_t mid = lo + (hi - lo) / 2;
+        if ((int64_t)ism_chunk_bytes(ix, IsmChunk{mid, B, mid + l - 1}) <= workspace_bytes) {
+            np = mid;
+            lo = mid + 1;
+        } else {
+            hi = mid - 1;
         }
-        QueryArgs a = query_args(ix, rows, rc, l);
-        a.wq = ix->spec.weighted ? rw : nullptr;
-        a.raw = kset;
-        if ((s = query_launch<MODE_RAW>(ix, a, nitems * ISM_SETS, st)) != GKM_OK) break;
-        GKM_PREFER_SHARED(ism_index_finish);
-        ism_index_finish<<<(unsigned)nitems, 256, 0, st>>>(kset, S, fwd, counts, B, W, L, l, p0, ref_raw, ref_score,
-                                                           inv_dx, inv_dmut, inv_ds, coef, gamma, rbf, out);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) s = gkm_cuda_status(e, "ism_index_finish");
     }
-    cudaFreeAsync(rows, st);
-    cudaFreeAsync(rc, st);
-    cudaFreeAsync(rw, st);
-    cudaFreeAsync(kset, st);
-    return s;
+    if (np == 0)
+        return gkm_fail(GKM_ERR_CAPACITY, "ISM workspace of %lld bytes holds no position (needs %lld)",
+                        (long long)workspace_bytes, (long long)ism_chunk_bytes(ix, IsmChunk{1, B, l}));
+    for (int64_t p0 = 0; p0 < L; p0 += np) {
+        const int64_t n_p = min(np, L - p0);
+        const IsmChunk ck{n_p, B, n_p + l - 1};
+        const int64_t rows = ck.rows();
+        if (rows > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many ISM rows in one chunk");
+        uint8_t *w = (uint8_t *)workspace;
+        uint32_t *qrows = (uint32_t *)w;
+        w += ism_align((size_t)rows * l * 4);
+        int32_t *qcnt = (int32_t *)w;
+        w += ism_align((size_t)rows * 4);
+        uint8_t *qwt = w;
+        w += ism_align((size_t)rows * l);
+        double *kbuf = (double *)w;
+        GKM_PREFER_SHARED(ism_rows_kernel);
+        ism_rows_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(ix->spec, fwd, counts, W, p0, ck, qrows, qcnt,
+                                                                        ix->spec.weighted ? qwt : nullptr);
+        GKM_CHECK_LAUNCH("ism_rows");
+        QueryArgs a = query_args(ix, qrows, qcnt, l);
+        a.wq = ix->spec.weighted ? qwt : nullptr;
+        a.raw = kbuf;
+        GKM_TRY(query_launch<MODE_RAW>(ix, a, rows, st));
+        GKM_PREFER_SHARED(ism_index_finish);
+        ism_index_finish<<<(unsigned)(n_p * B), 256, 0, st>>>(kbuf, S, fwd, counts, W, L, l, p0, ck, ref_raw,
+                                                             ref_score, inv_dmut, inv_ds, coef, gamma, rbf, out);
+        GKM_CHECK_LAUNCH("ism_index_finish");
+    }
+    return GKM_OK;
 }
 
 

@@ -271,7 +271,9 @@ class DeviceIndex:
         self.settle(before, run)
         return out
 
-    def pairwise(self, bx, cx, diag_offset=None, raw=True, profile=False, out=None):
+    def pairwise(self, bx, cx, diag_offset=None, raw=True, profile=False, out=None, check=True):
+        """(K_raw [B, S] or None, profiles [B, S, l+1] or None); check=False
+        skips the exactness check (no synchronisation: the caller settles)."""
         B, W = bx.shape
         if raw and out is None:
             out = torch.zeros((B, self.S), dtype=torch.float64, device=bx.device)
@@ -283,7 +285,7 @@ class DeviceIndex:
                  -1 if diag_offset is None else int(diag_offset), ptr(out if raw else None), ptr(prof), _st())
             return out, prof
 
-        return self.checked(run)
+        return self.checked(run) if check else run()
 
     def score(self, bx, cx, inv_dx, inv_ds, coef, gamma, rbf, bias, order=None, out=None, check=True):
         B, W = bx.shape

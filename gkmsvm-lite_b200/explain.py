@@ -160,7 +160,10 @@ def gkmexplain(model, x, *, mode="importance", lengths=None, batch_size=50, verb
     return per_position(out, batch, short)
 
 
-def _explain_rows(model, x, lengths, mode, dev, table=None):
+def _explain_rows(model, x, lengths, mode, dev, table=None, check=True):
+    """[B, 4, L] attributions of one pass (x: host or device codes).
+    check=False: no host synchronisation (the index's exactness check is the
+    caller's)."""
     kernel = model.kernel
     base = kernel.base
     spec = model._spec()
@@ -186,7 +189,7 @@ def _explain_rows(model, x, lengths, mode, dev, table=None):
              int(perturbation), ptr(out), stream_handle())
     elif isinstance(kernel, RbfKernel):
         index = model._sv_index()  # not None: _explain_uses_pairs
-        raw, _ = index.pairwise(fwd, counts)
+        raw, _ = index.pairwise(fwd, counts, check=check)
         inv_ds = model._inv_ds()
         k_norm = raw * inv_dx[:, None] * inv_ds[None, :]
         w = (model._sv_coef() * inv_ds)[None, :] * _rbf_scale(k_norm, kernel.gamma)

@@ -9,6 +9,8 @@ values and reduce over the SVs per mutant (gkm_index_mutants).
 
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
@@ -19,6 +21,8 @@ from .kernels import RbfKernel
 
 # Sequences per device pass: ISM outputs [B, 4, L] float64 per pass within this
 _BLOCK_BYTES = 1 * 2**30
+# Index-path ISM workspace (query rows and K_raw rows of a pass of positions)
+_WORKSPACE_BYTES = 3 * 2**29
 
 
 def ism(model, x, *, lengths=None, batch_size=None, verbose=False) -> torch.Tensor:
@@ -43,7 +47,9 @@ def ism(model, x, *, lengths=None, batch_size=None, verbose=False) -> torch.Tens
     return per_position(out, batch, short)
 
 
-def _ism_rows(model, x, lengths, dev):
+def _ism_rows(model, x, lengths, dev, check=True, work=None):
+    """[B, 4, L] deltas of one pass (x: host or device codes).  check=False:
+    no host synchronisation (the index's exactness check is the caller's)."""
     base = model.kernel.base
     spec = model._spec()
     L = x.shape[-1]
@@ -56,10 +62,10 @@ def _ism_rows(model, x, lengths, dev):
     if table is not None:
         _, raw, diag = engine.table_score(spec, table, fwd, rc, counts, 0.0, base.normalize, want_parts=True)
         return engine.ism_table(spec, table, fwd, counts, L, raw, diag, base.normalize)
-    return _ism_index(model, fwd, rc, counts, L)
+    return _ism_index(model, fwd, rc, counts, L, check, work)
 
 
-def _ism_index(model, fwd, rc, counts, L):
+def _ism_index(model, fwd, rc, counts, L, check=True, work=None):
     kernel = model.kernel
     base = kernel.base
     spec = model._spec()
@@ -78,14 +84,30 @@ def _ism_index(model, fwd, rc, counts, L):
     else:
         inv_dx = torch.ones(B, dtype=torch.float64, device=fwd.device)
         inv_dmut = torch.ones((4, L, B), dtype=torch.float64, device=fwd.device)
-    ref_raw, _ = index.pairwise(fwd, counts)
-    ref_score = index.score(fwd, counts, inv_dx, model._inv_ds(), model._sv_coef(), gamma, rbf, 0.0)
     out = torch.empty((B, 4, L), dtype=torch.float64, device=fwd.device)
+    if work is None:
+        work = ism_workspace(model, B, L, fwd.device)
 
     def run():
+        ref_raw, _ = index.pairwise(fwd, counts, check=False)
+        ref_score = index.score(fwd, counts, inv_dx, model._inv_ds(), model._sv_coef(), gamma, rbf, 0.0,
+                                check=False)
         call("gkm_index_mutants", index.handle, ptr(fwd), ptr(counts), B, W, L, ptr(ref_raw), ptr(ref_score),
              ptr(inv_dx), ptr(inv_dmut), ptr(model._inv_ds()), ptr(model._sv_coef()), float(gamma), int(rbf),
-             ptr(out), stream_handle())
+             ptr(out), ptr(work), int(work.numel()), stream_handle())
         return out
 
-    return index.checked(run)
+    return index.checked(run) if check else run()
+
+
+def ism_workspace_bytes(model, B: int, L: int, cap: int = None) -> int:
+    """Bytes of an index-path ISM workspace for B rows x L positions: the query
+    rows and K_raw rows of as many positions per chunk as fit in cap bytes
+    (at least one position's)."""
+    lo, hi = ctypes.c_int64(), ctypes.c_int64()
+    call("gkm_index_mutants_workspace", model._sv_index().handle, B, L, ctypes.byref(lo), ctypes.byref(hi))
+    return max(lo.value, min(hi.value, _WORKSPACE_BYTES if cap is None else cap))
+
+
+def ism_workspace(model, B: int, L: int, device, cap: int = None) -> torch.Tensor:
+    return torch.empty(ism_workspace_bytes(model, B, L, cap), dtype=torch.uint8, device=device)

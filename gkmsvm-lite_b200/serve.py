@@ -269,11 +269,17 @@ class GpuBackend:
 
     """Runs a GkmServer's batches on the model's GPU: scoring rows through
     BatchedScorer (two instances, one per in-flight slot, each on its own
-    stream), ISM and GkmExplain through the model's own calls on a side stream."""
+    high-priority stream), ISM and GkmExplain through BatchedIsm /
+    BatchedExplain bucket graphs on a low-priority side stream whose persistent
+    index queries take at most side_sm_share of the SMs."""
 
     # scoring batches of at most this many rows skip the graphs (DirectScorer):
     # the index query then splits their long rows over the whole GPU
     direct_rows = 64
+
+    # the side worker's persistent index queries take at most this share of
+    # the SMs, so a scoring pass launched meanwhile finds SMs free
+    side_sm_share = 0.5
 
     def __init__(self, model, slots: int = 2):
         import torch
@@ -286,8 +292,17 @@ class GpuBackend:
         model._sv_diag()
         self.scorers = [BatchedScorer(model) for _ in range(slots)]
         self.direct = [DirectScorer(model) for _ in range(slots)]
-        self.streams = [torch.cuda.Stream() for _ in range(slots)]
-        self.side_stream = torch.cuda.Stream()
+        # scoring passes are latency-bound requests: their streams get the
+        # highest priority, so their blocks are dispatched before pending
+        # blocks of the side stream's ISM / explain kernels
+        p = torch.cuda.Stream.priority_range()  # a lower number is a higher priority
+        self.streams = [torch.cuda.Stream(priority=min(p)) for _ in range(slots)]
+        self.side_stream = torch.cuda.Stream(priority=max(p))
+        props = torch.cuda.get_device_properties(model._device)
+        self.side_blocks = max(1, int(props.multi_processor_count * self.side_sm_share))
+        # ISM / GkmExplain in bucket-shaped CUDA graphs, one runner per kind
+        # (and explain mode), built by the side worker thread
+        self.side_runners: dict = {}
         self._slot = 0
         self._busy = [False] * slots
 
@@ -389,9 +404,6 @@ class GpuBackend:
         """One ISM or GkmExplain call over every row of reqs (same kind and
         mode), rows padded to the widest; each request gets its own rows at its
         own width (a row's results do not depend on the rows beside it)."""
-        from .explain import gkmexplain
-        from .ism import ism
-
         torch = self.torch
         L = max(int(np.asarray(r.x).shape[1]) for r in reqs)
         xs, lens, spans, a = [], [], [], 0
@@ -405,10 +417,19 @@ class GpuBackend:
             spans.append((a, n, w))
             a += n
         X, lengths = np.concatenate(xs), np.concatenate(lens)
+        from ._lib import call
+        from .batch import BatchedExplain, BatchedIsm
+
+        call("gkm_set_thread_grid_limit", int(self.side_blocks))  # this (side worker) thread only
+        key = "ism" if reqs[0].kind == "ism" else ("explain", reqs[0].mode)
+        runner = self.side_runners.get(key)
+        if runner is None:
+            runner = self.side_runners[key] = (BatchedIsm(self.model) if key == "ism"
+                                               else BatchedExplain(self.model, reqs[0].mode))
         with torch.cuda.stream(self.side_stream):
-            if reqs[0].kind == "ism":
-                res = ism(self.model, X, lengths=lengths)
-            else:
-                res = gkmexplain(self.model, X, lengths=lengths, mode=reqs[0].mode)
+            xd = torch.from_numpy(X).pin_memory().to(self.model._device, non_blocking=True)
+            ld = torch.from_numpy(lengths).pin_memory().to(self.model._device, non_blocking=True)
+            res = runner(xd, ld)
             host = res.cpu().numpy()
+        host[lengths < self.model.kernel.l] = np.nan  # rows with no window
         return [host[a:a + n, :, :w] for a, n, w in spans]

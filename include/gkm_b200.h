@@ -54,6 +54,12 @@ int gkm_version(void);
 const char *gkm_last_error(void);
 /* Number of SMs of the current device and its opt-in shared memory per block. */
 int gkm_device_info(int32_t *sm_count, int32_t *smem_per_block);
+/* Persistent index queries launched from the calling thread take at most
+ * `blocks` blocks (0: one per SM, the default).  Thread-local.  A serving loop
+ * gives its ISM / GkmExplain worker thread a limit so those long queries leave
+ * SMs to the scoring passes other threads launch.  No counterpart in
+ * gkmsvm-lite, which has no serving loop. */
+int gkm_set_thread_grid_limit(int32_t blocks);
 
 /* Packed forward and RC windows of [B, L] base codes; counts[b] = windows of
  * row b, lengths (nullable) = each row's length.
@@ -94,6 +100,13 @@ int gkm_dense_pairwise(const gkm_spec *spec, const uint32_t *bx, const int32_t *
                        int64_t B, int64_t Wx, const uint32_t *by, const uint32_t *ry,
                        const int32_t *cy, int64_t S, int64_t Wy, double *raw,
                        uint64_t *profile, int32_t *error, gkm_stream_t stream);
+/* Test hook: the limit (ns) of the dense kernel's waits on hand-offs between
+ * its roles (B record landed, accumulator ready or handed back), for the
+ * dense launches made from the calling thread; 0 restores the default 1 s.
+ * A wait that runs out sets the call's error flag; the kernel still waits
+ * (up to 1 s) for its copies and MMAs in flight and frees its tensor memory.
+ * No counterpart in gkmsvm-lite. */
+int gkm_dense_set_role_wait(int64_t ns);
 
 /* Builds the l-mer index over S columns (radix sort of the packed l-mers of
  * their forward and RC windows into per-SV-tile CSR buckets).  masks [n_masks]
@@ -207,14 +220,24 @@ int gkm_ism_table(const gkm_spec *spec, const double *table, const uint32_t *fwd
                   int32_t normalize, double *out, gkm_stream_t stream);
 
 /* ISM deltas [B, 4, L] through the index for any kernel (RBF included):
- * K(mutant, s) = ref_raw[b, s] + K(new windows, s) - K(old windows, s).
+ * K(mutant, s) = ref_raw[b, s] + K(new windows, s) - K(old windows, s), the
+ * old windows' term summed from one query row per reference window.
+ * inv_dmut [4, L, B]: 1 / sqrt(K(mutant, mutant)) (all 1 unnormalised).
+ * Allocates nothing: workspace (256-byte aligned, workspace_bytes) holds the
+ * query rows and K_raw rows of as many positions per pass as fit; it must
+ * hold at least gkm_index_mutants_workspace's min_bytes (GKM_ERR_CAPACITY
+ * otherwise); all_bytes does every position in one pass.  inv_dx is unused
+ * (kept for the operator's argument list).
  * Replaces LmerIndex.mutants (kernels/lmer_index.py:326-374,
  * kernels/lmer_index_cpu.py:203-285). */
+int gkm_index_mutants_workspace(const gkm_index_t *index, int64_t B, int64_t L, int64_t *min_bytes,
+                                int64_t *all_bytes);
 int gkm_index_mutants(const gkm_index_t *index, const uint32_t *fwd, const int32_t *counts,
                       int64_t B, int64_t W, int64_t L, const double *ref_raw,
                       const double *ref_score, const double *inv_dx,
-                      const double *mut_diag, const double *inv_ds, const double *coef,
-                      double gamma, int32_t rbf, double *out, gkm_stream_t stream);
+                      const double *inv_dmut, const double *inv_ds, const double *coef,
+                      double gamma, int32_t rbf, double *out, void *workspace,
+                      int64_t workspace_bytes, gkm_stream_t stream);
 
 /* scores[b] = sum_s coef[s] f(raw[b, s] / max(sqrt(dx[b] ds[s]), 1e-10)) + bias
  * over a materialised [B, S] block (dx, ds nullable: no normalisation).

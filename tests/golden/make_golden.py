@@ -120,26 +120,59 @@ def _model72k(kt, params):
     return GkmSVM(sv, coef, 0.0, kt, params, sv_lengths=svl)
 
 
+def config3_rows(xl, n_first=224, n_long=32, pool=20000):
+    """The first n_first queries of the config-3 stream and the n_long
+    longest of its first `pool` (2,000 bp rows included)."""
+    longest = np.argsort(-xl[:pool], kind="stable")
+    extra = [int(i) for i in longest if i >= n_first][:n_long]
+    return np.concatenate([np.arange(n_first), np.asarray(extra, np.int64)])
+
+
 def config3():
     xq, xl, _ = syn.config3_queries()
     out = {}
-    for name, kt, params, n in (
-        ("t2", "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, 256),
-        ("t3", "gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 2.0}, 48),
+    for name, kt, params, rows in (
+        ("t2", "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, np.arange(256)),
+        ("t3", "gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 2.0}, config3_rows(xl)),
     ):
         m = _model72k(kt, params)
         m.use_lmer_table = False
         t = time.time()
-        L = int(xl[:n].max())
-        out[f"{name}/scores"] = m(xq[:n, :L], lengths=xl[:n])
-        print(f"config3 {name} {n}: {time.time() - t:.1f}s", flush=True)
+        L = int(xl[rows].max())
+        out[f"{name}/scores"] = m(xq[rows, :L], lengths=xl[rows])
+        out[f"{name}/rows"] = rows
+        print(f"config3 {name} {len(rows)}: {time.time() - t:.1f}s", flush=True)
         if name == "t2":
             out["t2/diag_sv_head"] = np.asarray(m._sv_diag())[:256]
     np.savez_compressed(os.path.join(HERE, "config3.npz"), **out)
 
 
+ENCODE_MODEL = "encode_ENCFF579AOX.model.txt.gz"
+
+
+def encode():
+    """The full 72,145-SV ENCODE model (t2, l=11 k=7 d=3) the reference's
+    throughput benchmark scores (benchmarks/throughput_sweep.py:66-68), copied
+    beside the LS-GKM fixtures, with gkmsvm-lite's scores of 64 synthetic
+    300 bp queries (seed 6) for t2 and for the same SVs as gkmrbf gamma=1."""
+    from gkmsvm import load_model
+
+    dst = os.path.join(HERE, "lsgkm")
+    shutil.copy(os.path.join(REF_FIXTURES, ENCODE_MODEL), os.path.join(dst, ENCODE_MODEL))
+    x = syn.random_codes(np.random.default_rng(6), 64, 300)
+    full = load_model(os.path.join(dst, ENCODE_MODEL))
+    out = {"x": x}
+    t = time.time()
+    out["t2"] = full(x)
+    rbf = GkmSVM(full.support_sequences, full.coefficients, full.bias, "gkmrbf",
+                 {**full.kernel_params, "gamma": 1.0})
+    out["t3"] = rbf(x)
+    print(f"encode: {time.time() - t:.1f}s", flush=True)
+    np.savez_compressed(os.path.join(HERE, "encode.npz"), **out)
+
+
 def config4():
-    x = syn.config4_queries()[:2]
+    x = syn.config4_queries()[:16]
     m = _model72k("gkm_esttrunc", {"L": 11, "k": 7, "d": 3})
     t = time.time()
     out = {"ism": ref_ism(m, x)}
@@ -285,6 +318,6 @@ def deltasvm():
 
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "config1", "config2", "config3", "config4", "config5", "lsgkm", "deltasvm",
-                              "gkmsvm", "files"]
+                              "gkmsvm", "files", "encode"]
     for g in groups:
         globals()[g]()

@@ -125,3 +125,32 @@ def test_autotuner_times_once_per_class_and_changes_no_result(monkeypatch):
     monkeypatch.setattr(engine, "_time_form", timed_again)
     r2, _ = engine.pairwise(spec, bx, cx, by, ry, cy)
     assert torch.equal(r2, raw)
+
+
+def test_role_wait_running_out_raises_and_next_call_is_exact():
+    """A hand-off wait between the kernel's roles that runs out sets the
+    call's error flag: the kernel's roles leave their loops, its copies and
+    MMAs in flight are waited for (their own 1 s limit) and its tensor memory
+    is freed, so the call raises GkmError and the next normal call on the same
+    stream is bit-exact.  The role waits are shortened to 1 ns through the
+    test hook, so the first hand-off not complete on its first poll runs out."""
+    from gkmsvm_lite_b200._lib import call
+
+    kt, params, xl, yl = CASES["esttrunc_l11_long"]
+    rng = np.random.default_rng(3)
+    x, xl = _codes(rng, xl)
+    y, yl = _codes(rng, yl)
+    m = gk.GkmSVM(y, np.linspace(-1, 1, len(yl)), 0.0, kt, params, sv_lengths=yl).cuda()
+    spec = m._spec()
+    bx, _, cx = engine.pack(spec, torch.from_numpy(x).cuda(), xl)
+    by, ry, cy = m._sv_packed()
+    want, wprof = engine.join_pairwise(spec, bx, cx, by, ry, cy, profile=True)
+    call("gkm_dense_set_role_wait", 1)
+    try:
+        with pytest.raises(GkmError, match="wait limit"):
+            engine.dense_pairwise(spec, bx, cx, by, ry, cy)
+    finally:
+        call("gkm_dense_set_role_wait", 0)
+    raw, prof = engine.dense_pairwise(spec, bx, cx, by, ry, cy, profile=True)
+    torch.cuda.synchronize()
+    assert torch.equal(raw, want) and torch.equal(prof, wprof)

@@ -198,46 +198,115 @@ def test_config1_scores_match_reference():
 
 def test_config3_subsample_matches_reference():
     """72,000-SV model (SV lengths 200..500), queries 50..2000 bp with N: t=2
-    (256 queries) and t=3 gamma=2 (48 queries) against the reference."""
+    (the first 256 queries) and t=3 gamma=2 (256 queries: the first 224 and
+    the 32 longest of the first 20,000, 2,000 bp rows among them) against the
+    reference."""
     import gkmsvm_lite_b200.synthetic as syn
 
     sv, svl, coef = syn.config3_model()
     xq, xl, _ = syn.config3_queries()
     z = np.load(os.path.join(GOLDEN, "config3.npz"))
-    for name, kt, p, n in (("t2", "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, 256),
-                           ("t3", "gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 2.0}, 48)):
+    assert len(z["t3/rows"]) >= 256 and xl[z["t3/rows"]].max() >= 1990
+    for name, kt, p in (("t2", "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}),
+                        ("t3", "gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 2.0})):
+        rows = z[f"{name}/rows"]
         m = gk.GkmSVM(sv, coef, 0.0, kt, p, sv_lengths=svl).cuda()
         m.use_lmer_table = False
-        L = int(xl[:n].max())
-        got = _np(m(xq[:n, :L], lengths=xl[:n]))
+        L = int(xl[rows].max())
+        got = _np(m(xq[rows, :L], lengths=xl[rows]))
         np.testing.assert_allclose(got, z[f"{name}/scores"], rtol=RTOL, atol=ATOL)
         if name == "t2":
             np.testing.assert_allclose(_np(m._sv_diag())[:256], z["t2/diag_sv_head"], rtol=1e-12)
             m.use_lmer_table = True
-            np.testing.assert_allclose(_np(m(xq[:n, :L], lengths=xl[:n])), z["t2/scores"], rtol=RTOL, atol=ATOL)
+            np.testing.assert_allclose(_np(m(xq[rows, :L], lengths=xl[rows])), z["t2/scores"], rtol=RTOL,
+                                       atol=ATOL)
+
+
+def _config4_model():
+    import gkmsvm_lite_b200.synthetic as syn
+
+    sv, svl, coef = syn.config3_model()
+    return gk.GkmSVM(sv, coef, 0.0, "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, sv_lengths=svl).cuda()
 
 
 def test_config4_ism_matches_reference():
+    """16 x 1,000 bp through the l-mer table (fused mutant self-kernels) and
+    through the index (mutant window sets)."""
     import gkmsvm_lite_b200.synthetic as syn
 
-    sv, svl, coef = syn.config3_model()
-    x = syn.config4_queries()[:2]
+    x = syn.config4_queries()[:16]
     z = np.load(os.path.join(GOLDEN, "config4.npz"))
-    m = gk.GkmSVM(sv, coef, 0.0, "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, sv_lengths=svl).cuda()
-    m.use_lmer_table = True
-    got = _np(gk.ism(m, x))
-    np.testing.assert_allclose(got, z["ism"], rtol=RTOL, atol=1e-10 * np.abs(z["ism"]).max())
+    assert z["ism"].shape[0] == 16
+    m = _config4_model()
+    for table in (True, False):
+        m.use_lmer_table = table
+        got = _np(gk.ism(m, x))
+        np.testing.assert_allclose(got, z["ism"], rtol=RTOL, atol=1e-10 * np.abs(z["ism"]).max())
 
 
 def test_config4_explain_matches_reference():
+    """16 x 1,000 bp hypothetical attributions through the explain table and
+    through the l-mer neighbour path."""
     import gkmsvm_lite_b200.synthetic as syn
 
-    sv, svl, coef = syn.config3_model()
-    x = syn.config4_queries()[:2]
+    x = syn.config4_queries()[:16]
     z = np.load(os.path.join(GOLDEN, "config4.npz"))
-    m = gk.GkmSVM(sv, coef, 0.0, "gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, sv_lengths=svl).cuda()
-    got = _np(gk.gkmexplain(m, x, mode="hypothetical"))
-    np.testing.assert_allclose(got, z["explain_hyp"], rtol=RTOL, atol=1e-10 * np.abs(z["explain_hyp"]).max())
+    assert z["explain_hyp"].shape[0] == 16
+    m = _config4_model()
+    for table in ("auto", False):
+        m.use_explain_table = table
+        got = _np(gk.gkmexplain(m, x, mode="hypothetical", batch_size=16))
+        np.testing.assert_allclose(got, z["explain_hyp"], rtol=RTOL, atol=1e-10 * np.abs(z["explain_hyp"]).max())
+
+
+def test_encode_72k_model_matches_reference():
+    """The reference benchmark's 72,145-SV ENCODE model (LS-GKM text, loaded by
+    the native parser): gkmsvm-lite's scores of 64 x 300 bp queries for t2 (its
+    l-mer table and the index) and for the same SVs as gkmrbf gamma=1."""
+    z = np.load(os.path.join(GOLDEN, "encode.npz"))
+    m = gk.load_lsgkm_model(os.path.join(LSGKM, "encode_ENCFF579AOX.model.txt.gz")).cuda()
+    assert m.num_support_vectors == 72145
+    # near-zero scores of 72,145 summed terms: atol relative to the largest
+    # score (the reference's large-model tolerance, tests/test_gpu.py:783-784)
+    for table in (True, False):
+        m.use_lmer_table = table
+        np.testing.assert_allclose(_np(m(z["x"])), z["t2"], rtol=RTOL, atol=1e-10 * np.abs(z["t2"]).max())
+    r = gk.GkmSVM(m.support_sequences, m.coefficients, m.bias, "gkmrbf", {**m.kernel_params, "gamma": 1.0},
+                  sv_lengths=m.sv_lengths).cuda()
+    np.testing.assert_allclose(_np(r(z["x"])), z["t3"], rtol=RTOL, atol=1e-10 * np.abs(z["t3"]).max())
+
+
+def test_config2_profiles_sampled_pairs_bit_exact():
+    """Config 2 (4,000 sequences 100..1,000 bp, t=4 wgkm): mismatch profiles of
+    10,000 sampled (row, column) pairs through the index, the tensor-core form
+    and the join, and every diagonal (self-kernel), bit-exact against the
+    oracle."""
+    import gkmsvm_lite_b200.synthetic as syn
+
+    X, xl = syn.config2()
+    k = gk.CenterWeightedGkmKernel(11, 7, d=3)
+    kd = orc.KernelDef.from_params("wgkm", {"L": 11, "k": 7, "d": 3})
+    dev = torch.device("cuda")
+    spec = engine.Spec(k.base, dev)
+    bx, rx, cx = engine.pack(spec, torch.from_numpy(X).to(dev), xl)
+    rng = np.random.default_rng(8)
+    rows = np.sort(rng.choice(len(xl), 100, replace=False))
+    cols = np.stack([np.sort(rng.choice(len(xl), 100, replace=False)) for _ in rows])
+    want = np.stack([orc.profiles(X[r:r + 1], xl[r:r + 1], X[c], xl[c], kd)[0] for r, c in zip(rows, cols)])
+    ri = torch.from_numpy(rows).to(dev)
+    sub_x, sub_c = bx[ri].contiguous(), cx[ri].contiguous()
+    ix = engine.DeviceIndex(spec, bx, rx, cx, engine.masks_tensor(k.base, dev))
+    _, prof = ix.pairwise(sub_x, sub_c, raw=False, profile=True)
+    ix.close()
+    forms = {"index": _np(prof)}
+    for method in engine.pairwise_forms(spec):
+        forms[method] = _np(engine.pairwise(spec, sub_x, sub_c, bx, rx, cx, raw=False, profile=True,
+                                            method=method)[1])
+    for name, p in forms.items():
+        got = np.stack([p[i][cols[i]] for i in range(len(rows))])
+        np.testing.assert_array_equal(got.astype(np.uint64), want, err_msg=name)
+    _, diag = engine.self_kernel(spec, bx, rx, cx, profile=True)
+    np.testing.assert_array_equal(_np(diag).astype(np.uint64), orc.self_profiles(X, xl, kd, threads=os.cpu_count()))
 
 
 def test_config5_mixed_requests_match_reference():

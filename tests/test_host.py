@@ -166,6 +166,19 @@ def test_abi_library_exports_every_declared_symbol():
     assert lib.gkm_version() >= 1
 
 
+def test_thread_settings_refuse_negative_values():
+    """The serving grid limit and the dense kernel's role-wait test hook are
+    host-side, per-thread settings: negative values are refused, 0 restores
+    the default (no device work is involved)."""
+    from gkmsvm_lite_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.gkm_set_thread_grid_limit(-1) == _lib.GKM_ERR_INVALID
+    assert lib.gkm_set_thread_grid_limit(0) == _lib.GKM_OK
+    assert lib.gkm_dense_set_role_wait(-5) == _lib.GKM_ERR_INVALID
+    assert lib.gkm_dense_set_role_wait(0) == _lib.GKM_OK
+
+
 def test_pairwise_forms_and_classes():
     """The forms the autotuner chooses between (the tensor-core product only
     where dmax < l <= 15), and its shape classes."""

@@ -180,6 +180,24 @@ def test_encode_10sv_gkmpredict():
         assert abs(orc.scores(m, x)[0, 0] - float(want)) < 1e-4
 
 
+def test_encode_72k_model_index_baseline():
+    """The full 72,145-SV ENCODE model: the oracle's CPU index path (the bench's
+    CPU baseline) against gkmsvm-lite's t2 and gkmrbf gamma=1 scores of 64
+    synthetic 300 bp queries."""
+    z = np.load(os.path.join(GOLDEN, "encode.npz"))
+    m = orc.load_lsgkm(os.path.join(LSGKM, "encode_ENCFF579AOX.model.txt.gz"))
+    assert len(m.coef) == 72145
+    threads = os.cpu_count() or 1
+    for kt, params, key in (("gkm_esttrunc", {"L": 11, "k": 7, "d": 3}, "t2"),
+                            ("gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 1.0}, "t3")):
+        mk = orc.OracleModel(m.sv, m.sv_lengths, m.coef, m.bias, orc.KernelDef.from_params(kt, params))
+        got = orc.IndexBaseline(mk, threads=threads).scores(z["x"], threads=threads)
+        # summing 72,145 terms in another order leaves ~1e-11 on near-zero
+        # scores: atol relative to the largest score, as the reference's own
+        # large-model GPU tests do (tests/test_gpu.py:783-784)
+        np.testing.assert_allclose(got, z[key], rtol=1e-9, atol=1e-10 * np.abs(z[key]).max())
+
+
 @pytest.fixture(scope="module")
 def deltasvm_golden():
     z = np.load(os.path.join(GOLDEN, "deltasvm.npz"))
