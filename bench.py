@@ -310,15 +310,20 @@ def serving_leg(sv, svl, coef, n_requests=600, seed=4):
     t_closed = submit_all(srv)
     cap = srv.stats()
     srv.stop()
-    loads = {}
-    for frac in (0.5, 0.7):
+    # Poisson arrivals: three runs at 50 % of the closed-loop rate (other
+    # arrival draws), one at 70 %
+    runs50 = []
+    for _ in range(3):
         srv = GkmServer(backend).start()
-        submit_all(srv, frac * len(reqs) / t_closed)
-        st = srv.stats()
+        submit_all(srv, 0.5 * len(reqs) / t_closed)
+        runs50.append(srv.stats())
         srv.stop()
-        loads[frac] = st
+    srv = GkmServer(backend).start()
+    submit_all(srv, 0.7 * len(reqs) / t_closed)
+    loads = {0.5: runs50[0], 0.7: srv.stats()}
+    srv.stop()
     rate = 0.5 * len(reqs) / t_closed
-    open_stats = loads[0.5]
+    open_stats = max(runs50, key=lambda st: st["all"].get("p99_ms", 0.0))  # the worst of the three
     # plain per-call form: each request its own call, in order
     t0 = time.perf_counter()
     seqs = 0
@@ -343,6 +348,9 @@ def serving_leg(sv, svl, coef, n_requests=600, seed=4):
         "capacity_seqs_per_sec": cap["seqs_per_sec"], "capacity_requests_per_sec": len(reqs) / t_closed,
         "poisson_rate_requests_per_sec": rate,
         "p50_ms": open_stats["all"].get("p50_ms"), "p99_ms": open_stats["all"].get("p99_ms"),
+        "runs_at_50pct": [{"p50_ms": st["all"].get("p50_ms"), "p99_ms": st["all"].get("p99_ms"),
+                           "seqs_per_sec": st["seqs_per_sec"]} for st in runs50],
+        "headline_run": "the run of the three at 50 % with the highest p99",
         "by_kind_ms": {k: open_stats[k] for k in ("predict", "score_variants", "ism", "explain")},
         "served_seqs_per_sec": open_stats["seqs_per_sec"],
         "at_70pct_load": {"rate_requests_per_sec": 0.7 * len(reqs) / t_closed,
