@@ -415,7 +415,52 @@ def ism_explain_leg(sv, svl, coef, n=512):
     model.use_lmer_index = True
     model.use_explain_table = "auto"
     out["ism_path"] = "l-mer table + fused mutant self-kernels" if model._lmer_table is not None else "index"
+    out["ism_index_t5"] = ism_index_leg(sv, svl, coef)
     out["explain_path"] = "explain table (GPU Walsh-Hadamard build, cached)" if model._explain_tables else "l-mer neighbours"
+    return out
+
+
+def ism_index_leg(sv, svl, coef, rows=32, L=1000, seed=13):
+    """ISM through the l-mer index (the path RBF models take: mutant window
+    sets over the persistent index query) on the 72k-SV t=5 model of the
+    serving mix: rows x L bp through ism() and through the graph-captured
+    BatchedIsm (second call, graphs captured)."""
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+    import gkmsvm_lite_b200.synthetic as syn
+    from gkmsvm_lite_b200.batch import BatchedIsm
+
+    model = gk.GkmSVM(sv, coef, 0.0, "wgkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 1.0}, sv_lengths=svl).cuda()
+    x = syn.random_codes(np.random.default_rng(seed), rows, L)
+    gk.ism(model, x[:2])
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"workload": f"{rows} x {L} bp, 72,000-SV t=5 wgkmrbf gamma=1 model (index path)"}
+    torch.cuda.synchronize()
+    a.record()
+    want = gk.ism(model, x)
+    b.record()
+    torch.cuda.synchronize()
+    out["ism"] = {"value": rows / (a.elapsed_time(b) / 1e3), "unit": "seqs/sec", "ms_per_row": a.elapsed_time(b) / rows}
+    runner = BatchedIsm(model)
+    xd = torch.from_numpy(x).cuda()
+    runner(xd)
+    torch.cuda.synchronize()
+    a.record()
+    got = runner(xd)
+    b.record()
+    torch.cuda.synchronize()
+    out["batched_ism"] = {"value": rows / (a.elapsed_time(b) / 1e3), "unit": "seqs/sec",
+                          "ms_per_row": a.elapsed_time(b) / rows,
+                          "max_abs_diff_vs_ism": float((got - want).abs().max().item())}
+    single = x[:1]
+    gk.ism(model, single)
+    torch.cuda.synchronize()
+    a.record()
+    gk.ism(model, single)
+    b.record()
+    torch.cuda.synchronize()
+    out["single_row_ms"] = a.elapsed_time(b)
     return out
 
 
