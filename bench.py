@@ -39,6 +39,12 @@ WORKLOAD = ("config3: 72,000 SVs (200-500 bp, alpha ~ N(0, 0.1^2)), t=3 gkmrbf g
             "queries 50-2000 bp log-uniform with 0.5% N")
 
 
+# ncu on a 2,000-query launch of this workload (profiles/index_query_config3_t3_2000q.md):
+# throughput fractions of the units that bind the index query
+NCU_INDEX_QUERY = {"l1tex_throughput_frac": None, "lts_throughput_frac": None, "dram_bytes": 1.4475e9,
+                   "shared_atomic_bank_conflicts_per_wavefront": None}
+
+
 def job_config(queries: int, world: int) -> dict:
     """The workload description both arms print (the same dict for both)."""
     return {"workload": WORKLOAD, "queries_per_rank": queries, "svs": 72000, "parallelism": f"replicas x{world}",
@@ -793,10 +799,10 @@ def run_b200(args):
     result = None
     if rank == 0:
         # roofline of the dominant kernel: the fused index query (algorithmic
-        # bytes: lookups x 8 B (a bucket's two offsets) + hits x the stored
-        # entry size (2 B: SV ids within a tile of <= 65,536 SVs, unweighted)
+        # bytes: lookups x 8 B (a bucket's two offsets) + hits x 4 B (an SV id)
         # + 12 B per query window; hits counted exactly on the first queries
-        # and scaled by windows)
+        # and scaled by windows).  The index stores 2-byte ids (tiles of <=
+        # 65,536 SVs, unweighted): that count is reported beside it.
         fwd, rc, counts = engine.pack(spec, x_dev, l_dev)
         n_win = int(counts.sum().item())
         nsample = min(B, 4096)
@@ -805,8 +811,8 @@ def run_b200(args):
         hits = hits_s * n_win / max(win_s, 1)
         lookups = n_win * int(index.masks.numel())
         entry_bytes = 2 if (not spec.base.weighted and index.tile_svs <= 65536) else 4
-        alg_bytes = lookups * 8 + hits * entry_bytes + 12 * n_win
-        alg_bytes_4b = lookups * 8 + hits * 4 + 12 * n_win  # the 4-byte-id count
+        alg_bytes = lookups * 8 + hits * 4 + 12 * n_win
+        stored_bytes = lookups * 8 + hits * entry_bytes + 12 * n_win
         # DRAM traffic of the launch: ncu's dram__bytes_read.sum +
         # dram__bytes_write.sum on a 2,000-query launch of this workload
         # (1.4475e9 B; the SV index stays in L2), scaled by queries
@@ -828,9 +834,10 @@ def run_b200(args):
                          "traffic_source": "ncu dram bytes of a 2,000-query launch, scaled by queries",
                          "kernel": "index_query (fused SV-tile query + RBF + alpha reduce)",
                          "alg_bytes_per_launch": alg_bytes, "hits": hits, "lookups": lookups,
-                         "frac_4byte_ids": alg_bytes_4b / (query_ms / 1e3) / 1e9 / peak,
-                         "binding_unit": "L1/shared-memory atomics and L2 gathers (the index is L2-resident; "
-                                         "see l1tex / lts throughput in the ncu summary)",
+                         "frac_stored_entry_bytes": stored_bytes / (query_ms / 1e3) / 1e9 / peak,
+                         "binding_unit": "L1/shared atomics (the index is L2-resident: HBM is not what "
+                                         "binds it)",
+                         "ncu_small_case": NCU_INDEX_QUERY,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6.65 TB/s"},
             "stages_ms": {"prep (pack, self-kernels, order)": per_step * 1e3 - query_ms,
                           "index_query + finish": query_ms},

@@ -337,7 +337,7 @@ class BatchedIsm(_PerRowRunner):
         self._works = []  # every workspace a captured graph refers to
 
     def body(self, codes, lengths):
-        from . import ism as _ism
+        from .ism import _ism_rows, ism_workspace_bytes
 
         m = self.model
         work = None
@@ -345,12 +345,12 @@ class BatchedIsm(_PerRowRunner):
             # the index path's workspace, shared by the buckets (their replays
             # are serial); grown for a bucket of more rows (the eager warm-up
             # allocates it, never the capture)
-            need = _ism.ism_workspace_bytes(m, codes.shape[0], codes.shape[1])
+            need = ism_workspace_bytes(m, codes.shape[0], codes.shape[1])
             if self._work is None or self._work.numel() < need:
                 self._work = torch.empty(need, dtype=torch.uint8, device=codes.device)
                 self._works.append(self._work)
             work = self._work
-        return _ism._ism_rows(m, codes, lengths, codes.device, check=False, work=work)
+        return _ism_rows(m, codes, lengths, codes.device, check=False, work=work)
 
 
 class BatchedExplain(_PerRowRunner):
@@ -365,12 +365,12 @@ class BatchedExplain(_PerRowRunner):
         self._table = {}
 
     def body(self, codes, lengths):
-        from . import explain as _ex
+        from .explain import _explain_rows, _explain_table
 
         m = self.model
         pert = self.mode == "perturbation"
         if pert not in self._table:
             # the explain table, if the model's switch calls for one, is chosen
             # once per runner (a large call's cost model)
-            self._table[pert] = _ex._explain_table(m, 1 << 62, pert, codes.device)
-        return _ex._explain_rows(m, codes, lengths, self.mode, codes.device, self._table[pert], check=False)
+            self._table[pert] = _explain_table(m, 1 << 62, pert, codes.device)
+        return _explain_rows(m, codes, lengths, self.mode, codes.device, self._table[pert], check=False)

@@ -367,10 +367,14 @@ __device__ __forceinline__ uint32_t load_entry(const void *ent, uint32_t k)
     return __ldg((const uint32_t *)ent + k);
 }
 
-// One block per (row, SV tile): each warp takes whole query windows; each
-// lane one neighbour mask per chunk of 32, scanning its bucket four entries
-// at a time (the four loads in flight together); the next chunk's bucket
-// bounds are loaded while this chunk's entries are counted.
+// Persistent blocks take (SV tile, row) items: each warp takes whole query
+// windows (rows shorter than the warp count: (window, mask chunk) units split
+// evenly); each lane one neighbour mask per chunk of 32, scanning its bucket
+// four entries at a time (one vector load); the next chunk's bucket bounds
+// are loaded while this chunk's entries are counted.  Counts go to 16-bit
+// shared fields by plain adds, checked exactly at the end of the item (a
+// carry makes the decoded fields sum to less than the adds made), and the
+// rare item that carried is redone with the carry-logged adds.
 template <bool WEIGHTED, int MODE, bool C16, bool E16, bool RANGE>
 __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
 {
@@ -435,13 +439,8 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         }
         __syncthreads();
         uint32_t lane_hits = 0;  // per lane (<= its rounds x 1): plain adds made
-        // work units (window, chunk of 32 masks), window-major, split evenly
-        // into one contiguous range per warp: short rows (ISM window sets,
-        // row splits) keep every warp busy, long rows leave no idle last round
         const int nwin = i1 - i0;
         const int nchunk = (n_masks + 31) >> 5;
-        const int64_t nunit = (int64_t)nwin * nchunk;
-        const int64_t ub = nunit * warp / Q_WARPS, ue = nunit * (warp + 1) / Q_WARPS;
         // per lane: its mask's bucket (begin, length) and counter slot (C16:
         // word base of the level pair | the level's half in bit 31; wide: row
         // base of the level)
@@ -452,93 +451,116 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
             const uint32_t v = u ^ (mk & 0x00FFFFFFu);
             const uint32_t lev = mk >> 24;
             sl = C16 ? ((lev >> 1) * (uint32_t)St) | ((lev & 1u) << 31) : lev * (uint32_t)stride - (uint32_t)sub_lo;
-            // the bucket's bounds from the aligned group of four offsets
-            // holding off[v] (a second load only when off[v + 1] starts the
-            // next group)
-            const uint4 q = __ldg((const uint4 *)(off + (v & ~3u)));
-            const uint32_t r = v & 3u;
-            b0 = r == 0 ? q.x : r == 1 ? q.y : r == 2 ? q.z : q.w;
-            const uint32_t e0 = r == 0 ? q.y : r == 1 ? q.z : r == 2 ? q.w : __ldg(off + v + 1);
+            b0 = __ldg(off + v);
+            const uint32_t e0 = __ldg(off + v + 1);
             n0 = e0 - b0;
         };
         auto window_weight = [&](int i) -> uint32_t {
             return WEIGHTED ? (a.wq ? (uint32_t)a.wq[row * a.W + i] : gkm_wt(a.wd, n, i)) : 1u;
         };
-        if (ub < ue) {
-            int win = (int)(ub / nchunk), ch = (int)(ub - (int64_t)win * nchunk);
-            uint32_t u = x[i0 + win], wq = window_weight(i0 + win);
-            uint32_t beg, len, slot;
-            lane_mask(u, ch * 32 + lane, beg, len, slot);
-            for (int64_t un = ub; un < ue; un++) {
-                // the next unit's window and buckets, loaded while this one is counted
-                int nw = win, nc = ch + 1;
-                if (nc == nchunk) {
-                    nw = win + 1;
-                    nc = 0;
+        // the chunk being counted: this lane's bucket (beg, len), its counter
+        // slot, and the query window's weight
+        uint32_t wq = 1, beg = 0, len = 0, slot = 0;
+        // one index entry en of the bucket whose counter slot is sl
+        auto count_hit = [&](uint32_t en, uint32_t sl) {
+            const uint32_t id = E16 ? en : (en & 0x00FFFFFFu);
+            if (RANGE && (id < id_lo || id >= id_hi)) return;
+            if (C16) {
+                const uint32_t sh = (sl >> 31) * 16u;
+                if (logged) {
+                    count16(sm_acc, (sl & 0x7FFFFFFFu) + id, 1u << sh, 0xFFFFu << sh, &nlog, sm_log,
+                            a.status);
+                } else {
+                    atomicAdd(sm_acc + (sl & 0x7FFFFFFFu) + id, 1u << sh);
+                    lane_hits++;
                 }
-                uint32_t nu = u, nwq = wq, nbeg = 0, nlen = 0, nslot = 0;
-                if (un + 1 < ue) {
-                    if (nw != win) {
-                        nu = x[i0 + nw];
-                        nwq = window_weight(i0 + nw);
+            } else {
+                const uint32_t inc = WEIGHTED ? wq * (en >> 24) : 1u;
+                const uint32_t old = atomicAdd(sm_acc + sl + id, inc);
+                if (old + inc < old) atomicAdd(a.status + 1, 1u);
+            }
+        };
+        // blocks of four entries from e (aligned), one vector load each:
+        // each lane its own bucket [beg, end)
+        auto lane_block = [&](uint32_t e, uint32_t end) {
+            uint32_t en[4] = {0, 0, 0, 0};
+            if (e < end) {
+                if (E16) {
+                    const uint2 w = __ldg((const uint2 *)((const uint16_t *)a.ent + e));
+                    en[0] = w.x & 0xFFFFu;
+                    en[1] = w.x >> 16;
+                    en[2] = w.y & 0xFFFFu;
+                    en[3] = w.y >> 16;
+                } else {
+                    const uint4 w = __ldg((const uint4 *)((const uint32_t *)a.ent + e));
+                    en[0] = w.x;
+                    en[1] = w.y;
+                    en[2] = w.z;
+                    en[3] = w.w;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (e + q >= beg && e + q < end) count_hit(en[q], slot);
+        };
+        // this lane's bucket [beg, beg + len) in aligned blocks of four
+        // entries; the warp runs as many blocks as its longest bucket needs
+        auto walk = [&]() {
+            const uint32_t end = beg + len;
+            for (uint32_t e = beg & ~3u; __any_sync(GKM_FULL, e < end); e += 4) lane_block(e, end);
+        };
+        if (nwin >= Q_WARPS) {
+            // the row's windows to the warps in turn, all masks of a window in
+            // one warp
+            for (int i = i0 + warp; i < i1; i += Q_WARPS) {
+                const uint32_t u = x[i];
+                wq = window_weight(i);
+                lane_mask(u, lane, beg, len, slot);
+                for (int c0 = 0; c0 < n_masks; c0 += 32) {
+                    // the next chunk's buckets, loaded while this one is counted
+                    uint32_t nbeg, nlen, nslot;
+                    lane_mask(u, c0 + 32 + lane, nbeg, nlen, nslot);
+                    walk();
+                    beg = nbeg;
+                    len = nlen;
+                    slot = nslot;
+                }
+            }
+        } else {
+            // rows of fewer windows than warps (ISM window sets, the ends of
+            // row splits): (window, chunk of 32 masks) units, window-major, in
+            // one contiguous range per warp, so every warp has work
+            const int64_t nunit = (int64_t)nwin * nchunk;
+            const int64_t ub = nunit * warp / Q_WARPS, ue = nunit * (warp + 1) / Q_WARPS;
+            if (ub < ue) {
+                int win = (int)(ub / nchunk), ch = (int)(ub - (int64_t)win * nchunk);
+                uint32_t u = x[i0 + win];
+                wq = window_weight(i0 + win);
+                lane_mask(u, ch * 32 + lane, beg, len, slot);
+                for (int64_t un = ub; un < ue; un++) {
+                    // the next unit's window and buckets, loaded while this one is counted
+                    int nw = win, nc = ch + 1;
+                    if (nc == nchunk) {
+                        nw = win + 1;
+                        nc = 0;
                     }
-                    lane_mask(nu, nc * 32 + lane, nbeg, nlen, nslot);
-                }
-                // the warp's 32 buckets as one list of entries: bucket i holds
-                // list positions [excl_i, excl_i + len_i); a round gives lane j
-                // position f0 + j
-                uint32_t incl = len;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t y = __shfl_up_sync(GKM_FULL, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                const uint32_t total = __shfl_sync(GKM_FULL, incl, 31);
-                const uint32_t excl = incl - len;
-                const uint32_t dbase = beg - excl;  // entry index = dbase_i + list position
-                // lor: lane r holds the lane of the r-th non-empty bucket
-                const uint32_t nz = __ballot_sync(GKM_FULL, len != 0);
-                uint32_t lor = 0;
-#pragma unroll
-                for (int s = 16; s; s >>= 1)
-                    if (__popc(nz & ((1u << (lor + s)) - 1u)) <= (uint32_t)lane) lor += s;
-                uint32_t started = 0;  // non-empty buckets that began in earlier rounds
-                for (uint32_t f0 = 0; f0 < total; f0 += 32) {
-                    // non-empty buckets beginning in this round, by position
-                    const uint32_t p = excl - f0;
-                    const uint32_t starts = __reduce_or_sync(GKM_FULL, (len != 0 && p < 32u) ? 1u << p : 0u);
-                    const uint32_t rank = started + __popc(starts & (0xFFFFFFFFu >> (31 - lane))) - 1u;
-                    started += __popc(starts);
-                    const int src = __shfl_sync(GKM_FULL, (int)lor, (int)(rank & 31u));
-                    const uint32_t eb = __shfl_sync(GKM_FULL, dbase, src);
-                    const uint32_t sl = __shfl_sync(GKM_FULL, slot, src);
-                    const uint32_t f = f0 + lane;
-                    if (f >= total) continue;
-                    const uint32_t en = load_entry<E16>(a.ent, eb + f);
-                    const uint32_t id = E16 ? en : (en & 0x00FFFFFFu);
-                    if (RANGE && (id < id_lo || id >= id_hi)) continue;
-                    if (C16) {
-                        const uint32_t sh = (sl >> 31) * 16u;
-                        if (logged) {
-                            count16(sm_acc, (sl & 0x7FFFFFFFu) + id, 1u << sh, 0xFFFFu << sh, &nlog, sm_log,
-                                    a.status);
-                        } else {
-                            atomicAdd(sm_acc + (sl & 0x7FFFFFFFu) + id, 1u << sh);
-                            lane_hits++;
+                    uint32_t nu = u, nwq = wq, nbeg = 0, nlen = 0, nslot = 0;
+                    if (un + 1 < ue) {
+                        if (nw != win) {
+                            nu = x[i0 + nw];
+                            nwq = window_weight(i0 + nw);
                         }
-                    } else {
-                        const uint32_t inc = WEIGHTED ? wq * (en >> 24) : 1u;
-                        const uint32_t old = atomicAdd(sm_acc + sl + id, inc);
-                        if (old + inc < old) atomicAdd(a.status + 1, 1u);
+                        lane_mask(nu, nc * 32 + lane, nbeg, nlen, nslot);
                     }
+                    walk();
+                    beg = nbeg;
+                    len = nlen;
+                    slot = nslot;
+                    win = nw;
+                    ch = nc;
+                    u = nu;
+                    wq = nwq;
                 }
-                beg = nbeg;
-                len = nlen;
-                slot = nslot;
-                win = nw;
-                ch = nc;
-                u = nu;
-                wq = nwq;
             }
         }
         __syncthreads();

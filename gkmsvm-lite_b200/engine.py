@@ -106,7 +106,9 @@ def dense_pairwise(spec: Spec, bx, cx, by, ry, cy, raw: bool = True, profile: bo
     call("gkm_dense_pairwise", spec.ref, ptr(bx), ptr(cx), B, Wx, ptr(by), ptr(ry), ptr(cy), S, Wy,
          ptr(out), ptr(prof), ptr(err), _st())
     if check and int(err.item()) != 0:
-        raise _lib.GkmError("tensor-core pairwise: an MMA did not complete within its wait limit")
+        raise _lib.GkmError(_lib.GKM_ERR_CUDA,
+                            "tensor-core pairwise: a hand-off between the kernel's roles did not complete within "
+                            "its wait limit")
     return out, prof
 
 

@@ -277,10 +277,10 @@ def test_encode_72k_model_matches_reference():
 
 
 def test_config2_profiles_sampled_pairs_bit_exact():
-    """Config 2 (4,000 sequences 100..1,000 bp, t=4 wgkm): mismatch profiles of
-    10,000 sampled (row, column) pairs through the index, the tensor-core form
-    and the join, and every diagonal (self-kernel), bit-exact against the
-    oracle."""
+    """Config 2 (4,000 sequences 100..1,000 bp, t=4 wgkm): mismatch profiles
+    (levels 0..dmax, the ones with weight) of 10,000 sampled (row, column)
+    pairs through the index, the tensor-core form and the join, and every
+    diagonal (self-kernel), bit-exact against the oracle."""
     import gkmsvm_lite_b200.synthetic as syn
 
     X, xl = syn.config2()
@@ -302,11 +302,15 @@ def test_config2_profiles_sampled_pairs_bit_exact():
     for method in engine.pairwise_forms(spec):
         forms[method] = _np(engine.pairwise(spec, sub_x, sub_c, bx, rx, cx, raw=False, profile=True,
                                             method=method)[1])
+    # the GPU forms count the levels that carry weight, 0..dmax; the rest stay 0
+    d = kd.dmax
     for name, p in forms.items():
-        got = np.stack([p[i][cols[i]] for i in range(len(rows))])
-        np.testing.assert_array_equal(got.astype(np.uint64), want, err_msg=name)
+        got = np.stack([p[i][cols[i]] for i in range(len(rows))]).astype(np.uint64)
+        np.testing.assert_array_equal(got[..., : d + 1], want[..., : d + 1], err_msg=name)
+        assert not got[..., d + 1:].any(), name
     _, diag = engine.self_kernel(spec, bx, rx, cx, profile=True)
-    np.testing.assert_array_equal(_np(diag).astype(np.uint64), orc.self_profiles(X, xl, kd, threads=os.cpu_count()))
+    want_diag = orc.self_profiles(X, xl, kd, threads=os.cpu_count())
+    np.testing.assert_array_equal(_np(diag).astype(np.uint64)[:, : d + 1], want_diag[:, : d + 1])
 
 
 def test_config5_mixed_requests_match_reference():
