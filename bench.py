@@ -41,8 +41,9 @@ WORKLOAD = ("config3: 72,000 SVs (200-500 bp, alpha ~ N(0, 0.1^2)), t=3 gkmrbf g
 
 # ncu on a 2,000-query launch of this workload (profiles/index_query_config3_t3_2000q.md):
 # throughput fractions of the units that bind the index query
-NCU_INDEX_QUERY = {"l1tex_throughput_frac": None, "lts_throughput_frac": None, "dram_bytes": 1.4475e9,
-                   "shared_atomic_bank_conflicts_per_wavefront": None}
+NCU_INDEX_QUERY = {"l1tex_throughput_frac": 0.732, "lts_throughput_frac": 0.361, "dram_bytes": 1.464e9,
+                   "shared_atomic_wavefronts_frac": 0.279, "shared_atomic_bank_conflicts_per_wavefront": 0.62,
+                   "issue_active_frac": 0.564, "warps_active_frac": 0.50}
 
 
 def job_config(queries: int, world: int) -> dict:
@@ -815,8 +816,8 @@ def run_b200(args):
         stored_bytes = lookups * 8 + hits * entry_bytes + 12 * n_win
         # DRAM traffic of the launch: ncu's dram__bytes_read.sum +
         # dram__bytes_write.sum on a 2,000-query launch of this workload
-        # (1.4475e9 B; the SV index stays in L2), scaled by queries
-        traffic = 1.4475e9 * B / 2000
+        # (NCU_INDEX_QUERY; the SV index stays in L2), scaled by queries
+        traffic = NCU_INDEX_QUERY["dram_bytes"] * B / 2000
         achieved = alg_bytes / (query_ms / 1e3) / 1e9
         peaks = {}
         try:

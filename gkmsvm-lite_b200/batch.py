@@ -27,6 +27,23 @@ from .kernels import RbfKernel
 _ROW_GRANULE = 1024
 
 
+def _capture_graph(graph, fn, pool=None):
+    """fn()'s CUDA work captured into graph in thread-local mode, on a capture
+    stream of the graph's own.  torch.cuda.graph() is not used: it
+    synchronises the whole device first (an error while another thread -- a
+    server's other worker -- is capturing) and shares one capture stream per
+    process between threads."""
+    cs = torch.cuda.Stream()
+    cs.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(cs):
+        graph.capture_begin(pool=pool, capture_error_mode="thread_local")
+        try:
+            fn()
+        finally:
+            graph.capture_end()
+    torch.cuda.current_stream().wait_stream(cs)
+
+
 def _bucket_len(L: int) -> int:
     b = 64
     while b < L:
@@ -88,8 +105,8 @@ class _Graph:
         with torch.cuda.stream(side):
             self._body()
         torch.cuda.current_stream().wait_stream(side)
-        # thread-local capture: other threads (a server's side stream) may keep
-        # issuing CUDA work meanwhile.  The cyclic garbage collector stays off
+        # thread-local capture (_capture_graph): other threads may keep issuing CUDA
+        # work meanwhile.  The cyclic garbage collector stays off
         # while a capture is open: freeing an unreachable object that holds
         # another CUDA graph or device memory is not permitted during capture
         # and would invalidate it (torch.cuda.graph collects just before).
@@ -97,11 +114,9 @@ class _Graph:
         gc.disable()
         try:
             self.g_prep = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(self.g_prep, capture_error_mode="thread_local"):
-                self._prep()
+            _capture_graph(self.g_prep, self._prep)
             self.g_query = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(self.g_query, pool=self.g_prep.pool(), capture_error_mode="thread_local"):
-                self._query()
+            _capture_graph(self.g_query, self._query, pool=self.g_prep.pool())
         finally:
             if enabled:
                 gc.enable()
@@ -277,8 +292,7 @@ class _PerRowGraph:
             gc.disable()
             try:
                 self.graph = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(self.graph, capture_error_mode="thread_local"):
-                    self._body()
+                _capture_graph(self.graph, self._body)
             finally:
                 if enabled:
                     gc.enable()

@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
             chk[0] = chk[1] = 0;
         }
         __syncthreads();
-        uint32_t lane_hits = 0;  // per lane (<= its rounds x 1): plain adds made
+        unsigned long long lane_hits = 0;  // plain adds this lane made
         const int nwin = i1 - i0;
         const int nchunk = (n_masks + 31) >> 5;
         // per lane: its mask's bucket (begin, length) and counter slot (C16:
@@ -461,53 +461,69 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         // the chunk being counted: this lane's bucket (beg, len), its counter
         // slot, and the query window's weight
         uint32_t wq = 1, beg = 0, len = 0, slot = 0;
-        // one index entry en of the bucket whose counter slot is sl
-        auto count_hit = [&](uint32_t en, uint32_t sl) {
+        // one index entry en of this lane's bucket: counter word base + id
+        // (C16: add `add` to it, the level's 16-bit field; wide: row base)
+        auto count_hit = [&](uint32_t en, uint32_t base, uint32_t add) {
             const uint32_t id = E16 ? en : (en & 0x00FFFFFFu);
             if (RANGE && (id < id_lo || id >= id_hi)) return;
             if (C16) {
-                const uint32_t sh = (sl >> 31) * 16u;
                 if (logged) {
-                    count16(sm_acc, (sl & 0x7FFFFFFFu) + id, 1u << sh, 0xFFFFu << sh, &nlog, sm_log,
-                            a.status);
+                    count16(sm_acc, base + id, add, add * 0xFFFFu, &nlog, sm_log, a.status);
                 } else {
-                    atomicAdd(sm_acc + (sl & 0x7FFFFFFFu) + id, 1u << sh);
-                    lane_hits++;
+                    atomicAdd(sm_acc + base + id, add);
+                    if (RANGE) lane_hits++;  // else the chunk's bucket length is counted whole
                 }
             } else {
                 const uint32_t inc = WEIGHTED ? wq * (en >> 24) : 1u;
-                const uint32_t old = atomicAdd(sm_acc + sl + id, inc);
+                const uint32_t old = atomicAdd(sm_acc + base + id, inc);
                 if (old + inc < old) atomicAdd(a.status + 1, 1u);
             }
         };
-        // blocks of four entries from e (aligned), one vector load each:
-        // each lane its own bucket [beg, end)
-        auto lane_block = [&](uint32_t e, uint32_t end) {
-            uint32_t en[4] = {0, 0, 0, 0};
-            if (e < end) {
-                if (E16) {
-                    const uint2 w = __ldg((const uint2 *)((const uint16_t *)a.ent + e));
-                    en[0] = w.x & 0xFFFFu;
-                    en[1] = w.x >> 16;
-                    en[2] = w.y & 0xFFFFu;
-                    en[3] = w.y >> 16;
-                } else {
-                    const uint4 w = __ldg((const uint4 *)((const uint32_t *)a.ent + e));
-                    en[0] = w.x;
-                    en[1] = w.y;
-                    en[2] = w.z;
-                    en[3] = w.w;
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (e + q >= beg && e + q < end) count_hit(en[q], slot);
-        };
+#ifndef GKM_WALK_BLOCKS
+#define GKM_WALK_BLOCKS 2
+#endif
         // this lane's bucket [beg, beg + len) in aligned blocks of four
-        // entries; the warp runs as many blocks as its longest bucket needs
+        // entries, GKM_WALK_BLOCKS blocks per iteration with all their loads in
+        // flight before any is counted; the warp runs as many iterations as
+        // its longest bucket needs
         auto walk = [&]() {
+            constexpr int NB = GKM_WALK_BLOCKS;
             const uint32_t end = beg + len;
-            for (uint32_t e = beg & ~3u; __any_sync(GKM_FULL, e < end); e += 4) lane_block(e, end);
+            const uint32_t base = C16 ? slot & 0x7FFFFFFFu : slot, add = C16 ? 1u << ((slot >> 31) * 16u) : 0u;
+            if (!RANGE) lane_hits += len;
+            for (uint32_t e = beg & ~3u; __any_sync(GKM_FULL, e < end); e += 4 * NB) {
+                uint32_t en[4 * NB];
+                if (E16) {
+                    uint2 w[NB];
+#pragma unroll
+                    for (int k = 0; k < NB; k++)
+                        w[k] = e + 4 * k < end ? __ldg((const uint2 *)((const uint16_t *)a.ent + e + 4 * k))
+                                               : make_uint2(0, 0);
+#pragma unroll
+                    for (int k = 0; k < NB; k++) {
+                        en[4 * k] = w[k].x & 0xFFFFu;
+                        en[4 * k + 1] = w[k].x >> 16;
+                        en[4 * k + 2] = w[k].y & 0xFFFFu;
+                        en[4 * k + 3] = w[k].y >> 16;
+                    }
+                } else {
+                    uint4 w[NB];
+#pragma unroll
+                    for (int k = 0; k < NB; k++)
+                        w[k] = e + 4 * k < end ? __ldg((const uint4 *)((const uint32_t *)a.ent + e + 4 * k))
+                                               : make_uint4(0, 0, 0, 0);
+#pragma unroll
+                    for (int k = 0; k < NB; k++) {
+                        en[4 * k] = w[k].x;
+                        en[4 * k + 1] = w[k].y;
+                        en[4 * k + 2] = w[k].z;
+                        en[4 * k + 3] = w[k].w;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4 * NB; q++)
+                    if (e + q >= beg && e + q < end) count_hit(en[q], base, add);
+            }
         };
         if (nwin >= Q_WARPS) {
             // the row's windows to the warps in turn, all masks of a window in
