@@ -264,7 +264,7 @@ def run_reference(args):
     return 0
 
 
-def serving_leg(sv, svl, coef, n_requests=600, seed=4):
+def serving_leg(sv, svl, coef, n_requests=600, seed=4, backend_kw=None):
     """Config 5: the 72k-SV t=5 (wgkmrbf, gamma=1) model served with continuous
     batching.  Mixed requests (60% predict, 25% score-variants, 10% ISM, 5%
     GkmExplain), lengths log-uniform 20..2000 bp, alt = one SNV (80%) or an
@@ -291,7 +291,7 @@ def serving_leg(sv, svl, coef, n_requests=600, seed=4):
         if kind == "score_variants":
             r["alt"], r["alt_lengths"] = syn.variant_pairs(rng, x, ln)
         reqs.append(r)
-    backend = GpuBackend(model)
+    backend = GpuBackend(model, **(backend_kw or {}))
 
     def submit_all(srv, rate=None):
         futs = []
@@ -440,7 +440,7 @@ def ism_index_leg(sv, svl, coef, rows=32, L=1000, seed=13):
 
     model = gk.GkmSVM(sv, coef, 0.0, "wgkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 1.0}, sv_lengths=svl).cuda()
     x = syn.random_codes(np.random.default_rng(seed), rows, L)
-    gk.ism(model, x[:2])
+    gk.ism(model, x)  # the same shape: workspace and caches allocated
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {"workload": f"{rows} x {L} bp, 72,000-SV t=5 wgkmrbf gamma=1 model (index path)"}
     torch.cuda.synchronize()
@@ -528,8 +528,9 @@ ENCODE_PUBLISHED = {"t2": {"L40S": 45682, "A100": 35160}, "t3": {"L40S": 2202, "
 def encode_leg(n=1000, L=300, seed=6):
     """The reference's scoring-throughput benchmark shape (its
     benchmarks/throughput_sweep.py): the 72,145-SV ENCODE model read by the
-    native LS-GKM parser, as t2 (the file's gkm_esttrunc, default path: the
-    l-mer table) and with the same SVs as gkmrbf gamma=1 (t3, the l-mer index);
+    native LS-GKM parser, as t2 (the file's gkm_esttrunc: the path "auto"
+    picks for this call, and the l-mer table, the path the reference's own
+    run took) and with the same SVs as gkmrbf gamma=1 (t3, the l-mer index);
     n synthetic L bp queries as host one-hot [n, 4, L]; model(X) read back to
     the host, timed on the first call (SV caches built) and the second."""
     import torch
@@ -548,9 +549,11 @@ def encode_leg(n=1000, L=300, seed=6):
               base.kernel_params).cuda()(X[:32]).cpu()
     out = {"workload": f"72,145-SV ENCODE model (ENCFF579AOX, l=11 k=7 d=3), {n} synthetic {L} bp one-hot queries",
            "model_load_s": load_s, "published_seqs_per_sec": ENCODE_PUBLISHED}
-    for name, kt, extra in (("t2", "gkm_esttrunc", {}), ("t3", "gkmrbf", {"gamma": 1.0})):
+    for name, kt, extra, table in (("t2", "gkm_esttrunc", {}, "auto"), ("t2_table", "gkm_esttrunc", {}, True),
+                                   ("t3", "gkmrbf", {"gamma": 1.0}, "auto")):
         m = gk.GkmSVM(base.support_sequences, base.coefficients, base.bias, kt, {**base.kernel_params, **extra},
                       sv_lengths=base.sv_lengths).cuda()
+        m.use_lmer_table = table
         times = []
         for _ in range(3):
             torch.cuda.synchronize()
@@ -558,8 +561,9 @@ def encode_leg(n=1000, L=300, seed=6):
             m(X).cpu()
             times.append(time.perf_counter() - t0)
         path = "l-mer table" if m._lmer_table is not None and m._lmer_table is not False else "l-mer index"
+        pub = ENCODE_PUBLISHED[name.split("_")[0]]["L40S"]
         out[name] = {"first_s": times[0], "steady_s": min(times[1:]), "seqs_per_sec": n / min(times[1:]),
-                     "path": path, "vs_L40S": n / min(times[1:]) / ENCODE_PUBLISHED[name]["L40S"]}
+                     "path": path, "vs_L40S": n / min(times[1:]) / pub}
         del m
     return out
 
@@ -603,7 +607,7 @@ def pairwise_forms_leg(n_small=4000, rows=64, seed=12):
         m.use_lmer_table = False
         nwin = m._n_sv_windows()
         path = "index" if m._index_applies() else "all-pairs (autotuned)"
-        m(xq[:8, :L], lengths=xl[:8])  # builds the SV caches, tunes the pairwise form
+        m(xq[rowsel, :L], lengths=xl[rowsel])  # builds the SV caches, tunes the pairwise form
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()

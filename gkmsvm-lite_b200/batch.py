@@ -304,13 +304,17 @@ class _PerRowRunner:
     up to a multiple of row_granule, length to a power of two >= 64, so a few
     graphs serve batches of uneven length; each replay is one launch of the
     whole pass (packing, self-kernels, the persistent index queries over the
-    device work queue, the reductions).  Results equal the eager pass's."""
+    device work queue, the reductions).  A bucket runs eagerly on its first
+    use and is captured on its second, so one-off shapes pay no capture.
+    Results equal the eager pass's."""
 
     row_granule = 8
+    capture_after = 1  # eager runs of a bucket before it is captured
 
     def __init__(self, model):
         self.model = model
         self._graphs: dict = {}
+        self._uses: dict = {}
 
     def body(self, codes, lengths):  # [rows, 4, L] on the device, no host synchronisation
         raise NotImplementedError
@@ -333,7 +337,12 @@ class _PerRowRunner:
         else:
             g.lengths[:B].copy_(lengths)
         g.lengths[B:].zero_()
-        g.run()
+        uses = self._uses.get(key, 0)
+        self._uses[key] = uses + 1
+        if uses < self.capture_after:
+            g._body()
+        else:
+            g.run()
         if index is not None:
             # 16-bit counter carries that outgrew a block's log: rerun exactly
             index.settle(before, g._body)

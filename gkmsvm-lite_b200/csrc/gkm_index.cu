@@ -532,6 +532,22 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                 const uint32_t u = x[i];
                 wq = window_weight(i);
                 lane_mask(u, lane, beg, len, slot);
+#ifdef GKM_BOUNDS_AHEAD2
+                uint32_t b1, l1, s1;
+                lane_mask(u, 32 + lane, b1, l1, s1);
+                for (int c0 = 0; c0 < n_masks; c0 += 32) {
+                    // the buckets two chunks on, loaded while this one is counted
+                    uint32_t b2, l2, s2;
+                    lane_mask(u, c0 + 64 + lane, b2, l2, s2);
+                    walk();
+                    beg = b1;
+                    len = l1;
+                    slot = s1;
+                    b1 = b2;
+                    l1 = l2;
+                    s1 = s2;
+                }
+#else
                 for (int c0 = 0; c0 < n_masks; c0 += 32) {
                     // the next chunk's buckets, loaded while this one is counted
                     uint32_t nbeg, nlen, nslot;
@@ -541,6 +557,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                     len = nlen;
                     slot = nslot;
                 }
+#endif
             }
         } else {
             // rows of fewer windows than warps (ISM window sets, the ends of

@@ -24,6 +24,7 @@ from __future__ import annotations
 import queue
 import threading
 import time
+import warnings
 from concurrent.futures import Future
 from dataclasses import dataclass, field
 
@@ -277,11 +278,11 @@ class GpuBackend:
     # the index query then splits their long rows over the whole GPU
     direct_rows = 64
 
-    # the side worker's persistent index queries take at most this share of
-    # the SMs, so a scoring pass launched meanwhile finds SMs free
-    side_sm_share = 0.5
-
-    def __init__(self, model, slots: int = 2):
+    def __init__(self, model, slots: int = 2, side_sm_share: float = 0.5, side_graphs: bool = True):
+        """side_sm_share: the share of the SMs the side worker's persistent
+        index queries may take (1: all), so that a scoring pass launched
+        meanwhile finds SMs free; side_graphs: ISM / GkmExplain through the
+        bucketed graph runners (else direct ism() / gkmexplain() calls)."""
         import torch
 
         from .batch import BatchedScorer, DirectScorer
@@ -299,7 +300,8 @@ class GpuBackend:
         self.streams = [torch.cuda.Stream(priority=min(p)) for _ in range(slots)]
         self.side_stream = torch.cuda.Stream(priority=max(p))
         props = torch.cuda.get_device_properties(model._device)
-        self.side_blocks = max(1, int(props.multi_processor_count * self.side_sm_share))
+        self.side_blocks = 0 if side_sm_share >= 1 else max(1, int(props.multi_processor_count * side_sm_share))
+        self.side_graphs = side_graphs
         # ISM / GkmExplain in bucket-shaped CUDA graphs, one runner per kind
         # (and explain mode), built by the side worker thread
         self.side_runners: dict = {}
@@ -424,12 +426,24 @@ class GpuBackend:
         key = "ism" if reqs[0].kind == "ism" else ("explain", reqs[0].mode)
         runner = self.side_runners.get(key)
         if runner is None:
-            runner = self.side_runners[key] = (BatchedIsm(self.model) if key == "ism"
-                                               else BatchedExplain(self.model, reqs[0].mode))
+            if not self.side_graphs:
+                from .explain import gkmexplain
+                from .ism import ism as ism_call
+
+                runner = ((lambda x, ln: ism_call(self.model, x, lengths=ln)) if key == "ism" else
+                          (lambda x, ln, mode=reqs[0].mode: gkmexplain(self.model, x, lengths=ln, mode=mode)))
+            else:
+                runner = BatchedIsm(self.model) if key == "ism" else BatchedExplain(self.model, reqs[0].mode)
+            self.side_runners[key] = runner
         with torch.cuda.stream(self.side_stream):
-            xd = torch.from_numpy(X).pin_memory().to(self.model._device, non_blocking=True)
-            ld = torch.from_numpy(lengths).pin_memory().to(self.model._device, non_blocking=True)
-            res = runner(xd, ld)
+            if self.side_graphs:
+                xd = torch.from_numpy(X).pin_memory().to(self.model._device, non_blocking=True)
+                ld = torch.from_numpy(lengths).pin_memory().to(self.model._device, non_blocking=True)
+                res = runner(xd, ld)
+            else:
+                with warnings.catch_warnings():
+                    warnings.simplefilter("ignore")  # short rows: marked NaN below
+                    res = runner(X, lengths)
             host = res.cpu().numpy()
         host[lengths < self.model.kernel.l] = np.nan  # rows with no window
         return [host[a:a + n, :, :w] for a, n, w in spans]
