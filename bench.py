@@ -264,7 +264,7 @@ def run_reference(args):
     return 0
 
 
-def serving_leg(sv, svl, coef, n_requests=600, seed=4, backend_kw=None):
+def serving_leg(sv, svl, coef, n_requests=600, seed=4, backend_kw=None, server_kw=None):
     """Config 5: the 72k-SV t=5 (wgkmrbf, gamma=1) model served with continuous
     batching.  Mixed requests (60% predict, 25% score-variants, 10% ISM, 5%
     GkmExplain), lengths log-uniform 20..2000 bp, alt = one SNV (80%) or an
@@ -309,11 +309,11 @@ def serving_leg(sv, svl, coef, n_requests=600, seed=4, backend_kw=None):
             f.result(300)
         return time.perf_counter() - t0
 
-    warm = GkmServer(backend).start()
+    warm = GkmServer(backend, **(server_kw or {})).start()
     for r in reqs[:24]:
         warm.submit(r["kind"], r["x"], lengths=r["lengths"], alt=r.get("alt"), alt_lengths=r.get("alt_lengths")).result(600)
     warm.stop()
-    srv = GkmServer(backend).start()
+    srv = GkmServer(backend, **(server_kw or {})).start()
     t_closed = submit_all(srv)
     cap = srv.stats()
     srv.stop()
@@ -321,11 +321,11 @@ def serving_leg(sv, svl, coef, n_requests=600, seed=4, backend_kw=None):
     # arrival draws), one at 70 %
     runs50 = []
     for _ in range(3):
-        srv = GkmServer(backend).start()
+        srv = GkmServer(backend, **(server_kw or {})).start()
         submit_all(srv, 0.5 * len(reqs) / t_closed)
         runs50.append(srv.stats())
         srv.stop()
-    srv = GkmServer(backend).start()
+    srv = GkmServer(backend, **(server_kw or {})).start()
     submit_all(srv, 0.7 * len(reqs) / t_closed)
     loads = {0.5: runs50[0], 0.7: srv.stats()}
     srv.stop()
@@ -451,7 +451,8 @@ def ism_index_leg(sv, svl, coef, rows=32, L=1000, seed=13):
     out["ism"] = {"value": rows / (a.elapsed_time(b) / 1e3), "unit": "seqs/sec", "ms_per_row": a.elapsed_time(b) / rows}
     runner = BatchedIsm(model)
     xd = torch.from_numpy(x).cuda()
-    runner(xd)
+    for _ in range(2):  # the bucket's eager first use, then its capture
+        runner(xd)
     torch.cuda.synchronize()
     a.record()
     got = runner(xd)
@@ -576,15 +577,17 @@ def masked_join_hits(sv_windows: int, l: int, j: int, n_masks: int, q: float = 0
     return n_masks * sv_windows * q**j
 
 
-def pairwise_forms_leg(n_small=4000, rows=64, seed=12):
+def pairwise_forms_leg(n_small=4000, rows=128, seed=12):
     """The shapes where the reference would take its masked join: t=0 gkm_cnt
     l=11 k=7 with no d (dmax 4, 31,714 neighbour masks).  At the 72k-SV config-3
     model the index applies (11.7 indexed windows per l-mer lift its limit to
     32,768 neighbours, as the reference's kernels/lmer_index.py:97-109); with
-    n_small SVs of 300 bp it does not, and the autotuned all-pairs form (the
-    tensor-core product or the warp join) scores every window pair.  Beside
-    each: the masked join's own work, 330 masks of 7 kept positions (its plan
-    for h(m) = C(l - m, 7) is the single level j = 7)."""
+    n_small SVs of 300 bp the reference's rule would not, and the index is
+    taken where its measured cost is below the all-pairs forms'
+    (kernels.index_cost_below_pairs); the same rows also through the autotuned
+    all-pairs form (the tensor-core product or the warp join), which scores
+    every window pair.  Beside each: the masked join's own work, 330 masks of
+    7 kept positions (its plan for h(m) = C(l - m, 7) is the single level j = 7)."""
     import torch
 
     import gkmsvm_lite_b200 as gk
@@ -602,11 +605,13 @@ def pairwise_forms_leg(n_small=4000, rows=64, seed=12):
     rng = np.random.default_rng(seed)
     small = syn.random_codes(rng, n_small, 300)
     cases.append((f"{n_small}_svs_300bp", small, None, rng.normal(0, 0.1, n_small)))
+    cases.append((f"{n_small}_svs_300bp_all_pairs", small, None, cases[1][3]))
     for name, s_codes, s_len, s_coef in cases:
         m = gk.GkmSVM(s_codes, s_coef, 0.0, "gkm_cnt", params, sv_lengths=s_len).cuda()
         m.use_lmer_table = False
+        m.use_lmer_index = not name.endswith("all_pairs")
         nwin = m._n_sv_windows()
-        path = "index" if m._index_applies() else "all-pairs (autotuned)"
+        path = "index" if m._sv_index() is not None else "all-pairs (autotuned)"
         m(xq[rowsel, :L], lengths=xl[rowsel])  # builds the SV caches, tunes the pairwise form
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

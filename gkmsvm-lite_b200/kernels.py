@@ -89,6 +89,29 @@ def neighbor_count(l: int, dmax: int) -> int:
     return sum(comb(l, m) * 3**m for m in range(dmax + 1))
 
 
+# Costs per query window on B200 (the fused index query and the pairwise
+# forms, measured on the config-3 and t=0 workloads): an index lookup per SV
+# tile (neighbour masks read from global memory past the 6,144 that fit in
+# shared memory: about 3x), an index hit, and a window pair of the slower
+# all-pairs form at dmax >= 4 (~2e12 pairs/s).  SV tiles hold about 16M windows.
+_INDEX_LOOKUP_S = 2.6e-12
+_INDEX_HIT_S = 1.7e-12
+_PAIR_S = 5e-13
+_STAGED_MASKS = 6144
+_TILE_WINDOWS = 16_000_000
+
+
+def index_cost_below_pairs(l: int, n_neighbors: int, n_windows: int) -> bool:
+    """Whether the index costs less per query window than scoring every window
+    pair, for n_windows indexed windows: lookups per tile plus hits (the
+    expected share of windows within the neighbourhood, n_neighbors / 4^l, for
+    uniform bases) against n_windows pairs."""
+    tiles = 1 + n_windows // _TILE_WINDOWS
+    lookup = _INDEX_LOOKUP_S * (3 if n_neighbors > _STAGED_MASKS else 1)
+    index = n_neighbors * tiles * lookup + n_windows * (n_neighbors / 4**l) * _INDEX_HIT_S
+    return index < n_windows * _PAIR_S
+
+
 @lru_cache(maxsize=32)
 def neighbor_masks(l: int, nonzero: tuple, dmax: int) -> np.ndarray:
     """XOR masks of every l-mer within dmax mismatches of a window, levels m
@@ -183,12 +206,18 @@ class DirectGkmKernel(GkmKernel):
         return sum(comb(self.l, j) for j in range(self.l - dmax, self.l + 1)) <= _MAX_PLAN_MASKS
 
     def index_applies(self, n_windows: int | None = None) -> bool:
-        """kernels/lmer_index.py:97-109."""
+        """The reference's rule (kernels/lmer_index.py:97-109), and past it,
+        neighbourhoods up to DENSE_MAX_NEIGHBORS wherever the index's cost
+        per query window, measured on B200, is below the all-pairs forms'
+        (index_cost_below_pairs).  Every form gives the same K_raw."""
         if self.dmax < 0 or self.l > INDEX_MAX_L:
             return False
         count = neighbor_count(self.l, self.dmax)
         dense = n_windows is not None and n_windows >= DENSE_WINDOWS_PER_LMER * 4**self.l
-        return count <= (DENSE_MAX_NEIGHBORS if dense else MAX_NEIGHBORS)
+        if count <= (DENSE_MAX_NEIGHBORS if dense else MAX_NEIGHBORS):
+            return True
+        return count <= DENSE_MAX_NEIGHBORS and n_windows is not None and index_cost_below_pairs(
+            self.l, count, n_windows)
 
     def masks(self) -> np.ndarray:
         t = self._mismatch_table

@@ -443,7 +443,7 @@ def test_batched_scorer_equals_model(small, name, graphs):
     m = _model(c, use_lmer_table=False)
     x, xl = c["x"][:-1], c["x_lengths"][:-1]
     bs = BatchedScorer(m, use_graphs=graphs)
-    for _ in range(2):  # capture, then replay
+    for _ in range(3):  # eager, capture + replay, replay
         got = _np(bs.score(torch.from_numpy(x).cuda(), torch.from_numpy(xl).cuda()))
         np.testing.assert_allclose(got, c["scores"][:-1, 0], rtol=RTOL, atol=ATOL)
 
@@ -459,5 +459,35 @@ def test_batched_scorer_config1_table_and_index():
         m.use_lmer_table = table
         bs = BatchedScorer(m)
         x = torch.from_numpy(w.x).cuda()
-        for _ in range(2):
+        for _ in range(3):  # eager, capture + replay, replay
             np.testing.assert_allclose(_np(bs.score(x)), want, rtol=RTOL, atol=ATOL)
+
+
+def test_large_neighbourhood_index_past_reference_limit():
+    """t=0 gkm_cnt l=11 k=7 with no d (31,714 neighbour masks, read from global
+    memory) on 1,500 SVs: the index serves it (its measured cost is below the
+    all-pairs forms'), with profiles bit-exact to the tensor-core form and the
+    join and scores equal to the oracle's."""
+    import gkmsvm_lite_b200.synthetic as syn
+
+    rng = np.random.default_rng(31)
+    svl = rng.integers(200, 400, 1500)
+    sv = syn.ragged_codes(rng, svl)
+    coef = rng.normal(0, 0.2, 1500)
+    xl = rng.integers(30, 600, 12)
+    xl[0] = 599
+    x = syn.ragged_codes(rng, xl)
+    params = {"L": 11, "k": 7}
+    m = gk.GkmSVM(sv, coef, 0.1, "gkm_cnt", params, sv_lengths=svl).cuda()
+    m.use_lmer_table = False
+    assert m._sv_index() is not None and m._sv_index().masks.numel() == 31714
+    spec = m._spec()
+    fwd, rc, counts = engine.pack(spec, torch.from_numpy(x).cuda(), xl)
+    _, p_index = m._sv_index().pairwise(fwd, counts, raw=False, profile=True)
+    by, ry, cy = m._sv_packed()
+    for method in engine.pairwise_forms(spec):
+        _, p = engine.pairwise(spec, fwd, counts, by, ry, cy, raw=False, profile=True, method=method)
+        assert torch.equal(p, p_index), method
+    kd = orc.KernelDef.from_params("gkm_cnt", params)
+    want = orc.scores(orc.OracleModel(sv, svl, coef, 0.1, kd), x, xl)
+    np.testing.assert_allclose(_np(m(x, lengths=xl)), want, rtol=RTOL, atol=ATOL)

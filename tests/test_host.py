@@ -237,3 +237,18 @@ def test_pairwise_autotuner_caches_per_class(monkeypatch):
     assert engine.choose_pairwise(spec, i32(12, 1000), i32(12), cols, cols, ccount) == "dense"  # same class
     assert sorted(timed) == [("dense", 50), ("dense", 900), ("join", 50), ("join", 900)]
     assert len(engine.PAIRWISE_TUNED) == 2
+
+
+def test_index_rule_past_the_reference_limit():
+    """Neighbourhoods past the reference's limit (t=0 gkm_cnt l=11 k=7 with no
+    d: 31,714 masks) take the index where its measured cost per query window
+    is below the all-pairs forms' -- mid-size SV sets -- and not for a handful
+    of SVs; the reference's own cases are unchanged."""
+    k = K.DirectGkmKernel(11, 7)  # gkm_cnt, no d: dmax 4
+    assert K.neighbor_count(11, k.dmax) == 31714
+    assert not k.index_applies()
+    assert not k.index_applies(100 * 290 * 2)       # 100 SVs x 300 bp: every pair is cheaper
+    assert k.index_applies(4000 * 290 * 2)          # 4,000 SVs x 300 bp
+    assert k.index_applies(72000 * 340 * 2)         # the reference's dense-neighbourhood case
+    e = K.EstTruncGkmKernel(11, 7, d=3)             # 4,984 masks: always
+    assert e.index_applies() and e.index_applies(10)
