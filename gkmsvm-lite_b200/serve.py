@@ -64,13 +64,20 @@ class GkmServer:
     """Continuous-batching request loop over one model (see the module doc)."""
 
     def __init__(self, backend, *, max_batch_rows: int = 8192, max_inflight: int = 2,
-                 memory_reserve: int = 2 << 30, max_wait_s: float = 0.002, max_side_rows: int = 64):
+                 memory_reserve: int = 2 << 30, max_wait_s: float = 0.002, max_side_rows: int = 4,
+                 side_yield_s: float = 0.05):
+        """side_yield_s > 0: before each ISM / GkmExplain call the side worker
+        waits (at most this long) until no scoring pass is in flight or
+        waiting, so the two kinds of work share the GPU in time: a scoring
+        pass's index-query blocks take a whole SM's shared memory and can sit
+        behind a side call's kernels until they finish."""
         self.backend = backend
         self.max_batch_rows = max_batch_rows
         self.max_inflight = max_inflight
         self.memory_reserve = memory_reserve
         self.max_wait_s = max_wait_s
         self.max_side_rows = max_side_rows
+        self.side_yield_s = side_yield_s
         self.side_memory_wait_s = 30.0
         self.side_batches: list[int] = []  # requests per side call
         self._in: queue.Queue = queue.Queue()
@@ -234,6 +241,10 @@ class GkmServer:
                 for r in batch:
                     r.future.set_exception(AdmissionError("not enough free device memory for this request"))
                 continue
+            if self.side_yield_s > 0:
+                until = time.perf_counter() + self.side_yield_s
+                while (self._inflight or self._waiting or not self._in.empty()) and time.perf_counter() < until:
+                    time.sleep(0.0002)
             t = time.perf_counter()
             for r in batch:
                 r.t_start = t
@@ -278,7 +289,7 @@ class GpuBackend:
     # the index query then splits their long rows over the whole GPU
     direct_rows = 64
 
-    def __init__(self, model, slots: int = 2, side_sm_share: float = 0.5, side_graphs: bool = True):
+    def __init__(self, model, slots: int = 2, side_sm_share: float = 1.0, side_graphs: bool = True):
         """side_sm_share: the share of the SMs the side worker's persistent
         index queries may take (1: all), so that a scoring pass launched
         meanwhile finds SMs free; side_graphs: ISM / GkmExplain through the

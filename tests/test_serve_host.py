@@ -142,3 +142,37 @@ def test_side_request_beyond_free_memory_is_refused():
     np.testing.assert_array_equal(ok.result(10), np.full((2, 3), 2.0))
     srv.stop()
     assert srv.stats()["rejected"] == 1
+
+
+def test_side_worker_yields_to_scoring_passes():
+    """With side_yield_s, an ISM / explain call waits (bounded) until no
+    scoring pass is in flight or waiting, so the two share the GPU in time."""
+
+    class Recording(FakeBackend):
+        def __init__(self):
+            super().__init__(delay=0.15)
+            self.side_started_with_inflight = []
+
+        def run_side(self, r):
+            with self.lock:
+                self.side_started_with_inflight.append(self.inflight)
+            return np.asarray(r.x) * 2.0
+
+    be = Recording()
+    with GkmServer(be, max_inflight=2, memory_reserve=0, side_yield_s=1.0) as srv:
+        p = srv.submit("predict", np.ones((2, 5)))
+        time.sleep(0.02)  # the scoring pass is in flight when the ISM arrives
+        s = srv.submit("ism", np.ones((1, 5)))
+        assert s.result(10).shape == (1, 5) and p.result(10).shape == (2, 1)
+    assert be.side_started_with_inflight == [0]
+
+    # bounded: a side call never waits past side_yield_s
+    be = Recording()
+    be.delay = 5.0
+    with GkmServer(be, max_inflight=2, memory_reserve=0, side_yield_s=0.05) as srv:
+        srv.submit("predict", np.ones((2, 5)))
+        time.sleep(0.02)
+        t0 = time.perf_counter()
+        srv.submit("ism", np.ones((1, 5))).result(10)
+        assert time.perf_counter() - t0 < 2.0
+    assert be.side_started_with_inflight == [1]
