@@ -319,6 +319,40 @@ class GpuBackend:
         self._slot = 0
         self._busy = [False] * slots
 
+    def warm(self, max_len: int = 2048, max_rows: int = 8192, explain_modes=("hypothetical",)) -> None:
+        """Run and capture every graph bucket the loop can use (scoring rows in
+        multiples of 1,024 up to max_rows, side calls of max_side_rows, lengths
+        64..max_len) on rows of length 0, which have no windows and so almost
+        no work: a bucket's first use and its capture then never fall inside
+        a request's latency (the graphs do not depend on the rows' contents)."""
+        torch = self.torch
+        from .batch import BatchedExplain, BatchedIsm, _bucket_len
+
+        dev = self.model._device
+        lengths = [64]
+        while lengths[-1] < _bucket_len(max_len):
+            lengths.append(lengths[-1] * 2)
+        for i, scorer in enumerate(self.scorers):
+            with torch.cuda.stream(self.streams[i]):
+                for rows in range(1024, max_rows + 1, 1024):
+                    for L in lengths:
+                        x = torch.zeros((rows, L), dtype=torch.uint8, device=dev)
+                        ln = torch.zeros(rows, dtype=torch.int64, device=dev)
+                        for _ in range(2):
+                            scorer.score(x, ln)
+        with torch.cuda.stream(self.side_stream):
+            for key in ["ism"] + [("explain", m) for m in explain_modes]:
+                runner = self.side_runners.get(key)
+                if runner is None:
+                    runner = self.side_runners[key] = (BatchedIsm(self.model) if key == "ism"
+                                                       else BatchedExplain(self.model, key[1]))
+                for L in lengths:
+                    x = torch.zeros((runner.row_granule, L), dtype=torch.uint8, device=dev)
+                    ln = torch.zeros(runner.row_granule, dtype=torch.int64, device=dev)
+                    for _ in range(2):
+                        runner(x, ln)
+        torch.cuda.synchronize()
+
     def free_memory(self) -> int:
         """Bytes a new request can use: the device's free memory plus what
         torch's caching allocator holds but no tensor uses (it reuses that
