@@ -85,6 +85,28 @@ def estimated_lmer_table(l: int, k: int, truncate: bool) -> np.ndarray:
     return np.array(h, dtype=np.float64)
 
 
+@lru_cache(maxsize=64)
+def mask_plan(table: tuple, l: int, min_matches: int):
+    """The masked-join decomposition of a mismatch weight table (the
+    reference's kernels/masked.py:45-69): with dmax = l - min_matches, the
+    weights h(m), m <= dmax, as a sum over mask sizes j = l - dmax .. l of
+    a_j C(l - m, j) -- the number of size-j position subsets on which two
+    l-mers with m mismatches agree.  Returns [(j, a_j, positions [C(l, j), j]
+    int64)] for the sizes with a non-zero coefficient, or None when there is no
+    plan (no weight, or more than _MAX_PLAN_MASKS masks)."""
+    dmax = l - min_matches
+    if dmax < 0 or min_matches < 1:
+        return None
+    sizes = list(range(l - dmax, l + 1))
+    if sum(comb(l, j) for j in sizes) > _MAX_PLAN_MASKS:
+        return None
+    system = np.array([[comb(l - m, j) for j in sizes] for m in range(dmax + 1)], dtype=np.float64)
+    coef = np.linalg.solve(system, np.asarray(table, dtype=np.float64)[: dmax + 1])
+    floor = 1e-12 * np.abs(coef).max()
+    return [(j, float(c), np.array(list(combinations(range(l), j)), dtype=np.int64))
+            for j, c in zip(sizes, coef) if abs(c) > floor]
+
+
 def neighbor_count(l: int, dmax: int) -> int:
     return sum(comb(l, m) * 3**m for m in range(dmax + 1))
 
@@ -200,10 +222,11 @@ class DirectGkmKernel(GkmKernel):
     def has_table(self) -> bool:
         """Whether an exact l-mer table exists: the masked-join plan does
         (kernels/masked.py:142-167)."""
-        dmax = self.dmax
-        if dmax < 0 or self._min_matches < 1 or self.l > MAX_TABLE_L:
-            return False
-        return sum(comb(self.l, j) for j in range(self.l - dmax, self.l + 1)) <= _MAX_PLAN_MASKS
+        return self.l <= MAX_TABLE_L and self.mask_plan() is not None
+
+    def mask_plan(self):
+        """This kernel's masked-join plan (see mask_plan)."""
+        return mask_plan(tuple(float(v) for v in self._mismatch_table), self.l, self._min_matches)
 
     def index_applies(self, n_windows: int | None = None) -> bool:
         """The reference's rule (kernels/lmer_index.py:97-109), and past it,

@@ -147,6 +147,29 @@ def config3():
     np.savez_compressed(os.path.join(HERE, "config3.npz"), **out)
 
 
+MASK_PLAN_KERNELS = [(kt, params) for _, kt, params, *_ in SMALL] + [
+    ("gkm_esttrunc", {"L": 11, "k": 7, "d": 3}), ("gkm_cnt", {"L": 11, "k": 7}),
+    ("gkm_estfull", {"L": 10, "k": 6}), ("gkm_cnt", {"L": 12, "k": 8, "d": 2})]
+
+
+def maskplan():
+    """gkmsvm-lite's masked-join plans (kernels/masked.py:45-69): mask sizes and
+    coefficients of the small kernels and a few l = 10..12 ones."""
+    from gkmsvm.kernels.masked import mask_plan
+
+    out = {}
+    for i, (kt, params) in enumerate(MASK_PLAN_KERNELS):
+        base = GkmSVM(np.zeros((1, 20), np.uint8), np.ones(1), 0.0, kt, params).kernel.base
+        plan = mask_plan(tuple(float(v) for v in base._mismatch_table), base.l, base._min_matches)
+        out[f"{i}/kernel"] = np.array(f"{kt} {params!r}")
+        out[f"{i}/none"] = np.array(plan is None)
+        if plan is not None:
+            out[f"{i}/sizes"] = np.array([j for j, _, _ in plan])
+            out[f"{i}/coefs"] = np.array([c for _, c, _ in plan])
+            out[f"{i}/positions_sum"] = np.array([int(p.sum()) for _, _, p in plan])
+    np.savez_compressed(os.path.join(HERE, "maskplan.npz"), **out)
+
+
 ENCODE_MODEL = "encode_ENCFF579AOX.model.txt.gz"
 
 
@@ -318,6 +341,6 @@ def deltasvm():
 
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "config1", "config2", "config3", "config4", "config5", "lsgkm", "deltasvm",
-                              "gkmsvm", "files", "encode"]
+                              "gkmsvm", "files", "encode", "maskplan"]
     for g in groups:
         globals()[g]()

@@ -5,6 +5,7 @@ symbol include/gkm_b200.h declares."""
 import ctypes
 import os
 import re
+from math import comb
 
 import numpy as np
 import pytest
@@ -252,3 +253,30 @@ def test_index_rule_past_the_reference_limit():
     assert k.index_applies(72000 * 340 * 2)         # the reference's dense-neighbourhood case
     e = K.EstTruncGkmKernel(11, 7, d=3)             # 4,984 masks: always
     assert e.index_applies() and e.index_applies(10)
+
+
+def test_mask_plan_matches_reference():
+    """The masked-join plan (kernels/masked.py:45-69): mask sizes, coefficients
+    and position subsets equal gkmsvm-lite's for every small kernel type and a
+    few l = 10..12 kernels (tests/golden/maskplan.npz, made by make_golden.py),
+    and a plan exists exactly where the kernel reports an l-mer table."""
+    import ast
+
+    from conftest import GOLDEN
+
+    z = np.load(os.path.join(GOLDEN, "maskplan.npz"))
+    n = len({k.split("/")[0] for k in z.files})
+    assert n >= 10
+    for i in range(n):
+        kt, params = str(z[f"{i}/kernel"]).split(" ", 1)
+        base = gk.KERNEL_BUILDERS[K.resolve_kernel_type(kt)](ast.literal_eval(params)).base
+        plan = base.mask_plan()
+        assert (plan is None) == bool(z[f"{i}/none"]), (kt, params)
+        if plan is None:
+            continue
+        np.testing.assert_array_equal([j for j, _, _ in plan], z[f"{i}/sizes"])
+        np.testing.assert_allclose([c for _, c, _ in plan], z[f"{i}/coefs"], rtol=1e-12, atol=1e-15)
+        np.testing.assert_array_equal([int(p.sum()) for _, _, p in plan], z[f"{i}/positions_sum"])
+        for j, _, pos in plan:
+            assert pos.shape == (comb(base.l, j), j)
+        assert base.has_table() == (base.l <= K.MAX_TABLE_L)
