@@ -124,10 +124,12 @@ def parse():
     ap.add_argument("--queries", type=int, default=100000)
     ap.add_argument("--no-extras", action="store_true", help="skip t=2, plain-call and CPU legs")
     ap.add_argument("--leg", default="all",
-                    choices=["all", "gram", "train", "explain", "explain-pairs", "serve", "encode", "pairwise-forms"],
+                    choices=["all", "gram", "train", "explain", "explain-pairs", "serve", "encode", "pairwise-forms",
+                             "weighted"],
                     help="gram / train / explain: run only the Gram-matrix, SMO training or config-4 ISM and "
                          "GkmExplain leg (one GPU), print its JSON")
     ap.add_argument("--gram-n", type=int, default=4000, help="sequences of the Gram-matrix leg")
+    ap.add_argument("--weighted-n", type=int, default=20000, help="queries of the weighted (t=5) scoring leg")
     return ap.parse_args()
 
 
@@ -574,6 +576,58 @@ def encode_leg(n=1000, L=300, seed=6):
     return out
 
 
+def weighted_leg(n=20000, steps=3):
+    """Batched scoring with the weighted kernel of the serving mix: the 72k-SV
+    config-3 SVs as t=5 wgkmrbf gamma=1 (M=50, H=50), n config-3 queries,
+    through BatchedScorer; its index query counts in 32-bit shared counters
+    (window weights up to 50 x 50 per pair), so an SV tile holds 12,000 SVs (6
+    tiles, against 3 unweighted).  Roofline bytes: lookups x 8 B + hits x
+    (4 B id + 1 B weight) + 12 B per window."""
+    import torch
+
+    import gkmsvm_lite_b200 as gk
+    import gkmsvm_lite_b200.synthetic as syn
+    from gkmsvm_lite_b200 import engine
+    from gkmsvm_lite_b200.batch import BatchedScorer
+
+    sv, svl, coef = syn.config3_model()
+    xq, xl, _ = syn.config3_queries(n=n)
+    m = gk.GkmSVM(sv, coef, 0.0, "wgkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 1.0}, sv_lengths=svl).cuda()
+    index = m._sv_index()
+    x, ln = torch.from_numpy(xq).cuda(), torch.from_numpy(xl).cuda()
+    sc = BatchedScorer(m)
+    for _ in range(3):  # eager, capture, replay
+        sc.score(x, ln)
+    torch.cuda.synchronize()
+    ev = []
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        e = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        sc.score(x, ln, events=e, check=False)
+        ev.append(e)
+    b.record()
+    torch.cuda.synchronize()
+    sc.check_flags()
+    step_ms = a.elapsed_time(b) / steps
+    query_ms = float(np.mean([e0.elapsed_time(e1) for e0, e1 in ev]))
+    fwd, _, counts = engine.pack(m._spec(), x, ln)
+    n_win = int(counts.sum().item())
+    look, hits_s = index.count(fwd[:4096], counts[:4096])
+    hits = hits_s * n_win / max(int(counts[:4096].sum().item()), 1)
+    alg = n_win * int(index.masks.numel()) * 8 + hits * 5 + 12 * n_win
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    return {"workload": f"config-3 SVs as t=5 wgkmrbf gamma=1, {n} config-3 queries, batched",
+            "value": n / (step_ms / 1e3), "unit": "seqs/sec", "tiles": index.tiles, "tile_svs": index.tile_svs,
+            "query_ms": query_ms, "roofline": {"achieved_GBs": alg / (query_ms / 1e3) / 1e9, "peak_GBs": peak,
+                                               "frac": alg / (query_ms / 1e3) / 1e9 / peak, "hits": hits}}
+
+
 def masked_join_hits(sv_windows: int, l: int, j: int, n_masks: int, q: float = 0.2564) -> float:
     """Expected exact-match hits per query window of the reference's masked
     join (kernels/masked.py:45-69, 265-310) with n_masks masks keeping j of l
@@ -916,6 +970,7 @@ def run_b200(args):
                 result["gram"] = gram_leg(args.gram_n)
                 result["encode"] = encode_leg()
                 result["pairwise_forms"] = pairwise_forms_leg()
+                result["weighted_t5"] = weighted_leg()
                 result["training"] = training_leg(args.gram_n)
     if rank == 0:
         # the oracle re-scores rows of the timed batch (the longest, the most
@@ -964,6 +1019,9 @@ def main():
         import gkmsvm_lite_b200.synthetic as syn
 
         print(json.dumps(serving_leg(*syn.config3_model())), flush=True)
+        return 0
+    if args.leg == "weighted":
+        print(json.dumps(weighted_leg(args.weighted_n)), flush=True)
         return 0
     if args.leg == "pairwise-forms":
         print(json.dumps(pairwise_forms_leg()), flush=True)

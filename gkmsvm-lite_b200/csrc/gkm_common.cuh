@@ -117,6 +117,7 @@ struct gkm_index {
     int64_t bytes;
     int32_t acc_bytes;   // shared memory left for counters in a query block
     int32_t wide;        // 1: 32-bit counters (weighted, or after a carry-log overflow)
+    uint32_t wmax;       // largest window weight (1 unweighted)
     unsigned int *status; // [2] query event counts (see gkm_index_status)
     unsigned int *queues;            // [GKM_QUEUE_SLOTS] work-queue heads, one per call in flight
     mutable std::atomic<unsigned> next_queue{0};

@@ -8,6 +8,7 @@
 // tile's SVs in a fixed order (deterministic), so no [rows, S] block is written.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include "gkm_common.cuh"
 
@@ -289,6 +290,10 @@ struct QueryArgs {
     unsigned int *queue;  // work-queue head: items (tile, row) handed out tile-major
     int64_t B;            // rows
     int tiles;
+    // 32-bit counters: the most one query window can add to one counter (its
+    // SV's windows x the largest weight product); an item whose windows times
+    // this stays below 2^32 cannot wrap a counter, and adds without checking
+    uint64_t wide_bound;
     int nsplit;           // items per (row, tile): window ranges of split_w windows
     int split_w;
     unsigned long long *gcount;  // MODE_COUNT: [B, S, nlev] summed counts
@@ -318,10 +323,11 @@ __host__ __device__ inline size_t query_fixed_smem(int n_masks)
 // 32-bit word.  A field that passes 65535 carries into its neighbour (or out
 // of the word); the adder sees that in the value atomicAdd returns and logs
 // it, and the epilogue adds the carries back, so the counts stay exact.
-template <bool C16>
+template <bool C16, bool C64>
 __device__ __forceinline__ int64_t read_count(const uint32_t *acc, const uint32_t *log, int nlog, int m, int St,
                                               int s)
 {
+    if (C64) return (int64_t)((const unsigned long long *)acc)[m * St + s];
     if (!C16) return acc[m * St + s];
     // levels 2j and 2j+1 of SV s share word j * St + s (low and high half)
     const uint32_t word = (uint32_t)((m >> 1) * St + s), half = (uint32_t)(m & 1);
@@ -374,8 +380,10 @@ __device__ __forceinline__ uint32_t load_entry(const void *ent, uint32_t k)
 // are loaded while this chunk's entries are counted.  Counts go to 16-bit
 // shared fields by plain adds, checked exactly at the end of the item (a
 // carry makes the decoded fields sum to less than the adds made), and the
-// rare item that carried is redone with the carry-logged adds.
-template <bool WEIGHTED, int MODE, bool C16, bool E16, bool RANGE>
+// rare item that carried is redone with the carry-logged adds.  Wide counters
+// are 32-bit, or 64-bit (C64) for the rerun of a weighted call whose 32-bit
+// count wrapped.
+template <bool WEIGHTED, int MODE, bool C16, bool E16, bool RANGE, bool C64 = false>
 __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
 {
     extern __shared__ __align__(16) uint8_t smraw[];
@@ -432,7 +440,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         // only then the item is redone with the carry-logged adds
         bool logged = false;
         for (;;) {
-        for (int k = threadIdx.x; k < nacc; k += Q_THREADS) sm_acc[k] = 0;
+        for (int k = threadIdx.x; k < (C64 ? 2 * nacc : nacc); k += Q_THREADS) sm_acc[k] = 0;
         if (threadIdx.x == 0) {
             nlog = 0;
             chk[0] = chk[1] = 0;
@@ -440,6 +448,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         __syncthreads();
         unsigned long long lane_hits = 0;  // plain adds this lane made
         const int nwin = i1 - i0;
+        const bool wide_safe = !C16 && (unsigned long long)nwin * a.wide_bound < (1ull << 32);
         const int nchunk = (n_masks + 31) >> 5;
         // per lane: its mask's bucket (begin, length) and counter slot (C16:
         // word base of the level pair | the level's half in bit 31; wide: row
@@ -473,19 +482,28 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                     atomicAdd(sm_acc + base + id, add);
                     if (RANGE) lane_hits++;  // else the chunk's bucket length is counted whole
                 }
+            } else if (C64) {
+                atomicAdd((unsigned long long *)sm_acc + base + id,
+                          (unsigned long long)(WEIGHTED ? wq * (en >> 24) : 1u));
             } else {
                 const uint32_t inc = WEIGHTED ? wq * (en >> 24) : 1u;
-                const uint32_t old = atomicAdd(sm_acc + base + id, inc);
-                if (old + inc < old) atomicAdd(a.status + 1, 1u);
+                if (wide_safe) {
+                    atomicAdd(sm_acc + base + id, inc);
+                } else {
+                    const uint32_t old = atomicAdd(sm_acc + base + id, inc);
+                    if (old + inc < old) atomicAdd(a.status + 1, 1u);
+                }
             }
         };
         // this lane's bucket [beg, beg + len) in aligned blocks of four
-        // entries, four blocks per iteration with all their loads in flight
-        // before any is counted (measured: 2 blocks 417 ms, 3: 405, 4: 401 on
-        // 5,000 config-3 queries; one block 500); the warp runs as many
-        // iterations as its longest bucket needs
+        // entries, several blocks per iteration with all their loads in flight
+        // before any is counted; the warp runs as many iterations as its
+        // longest bucket needs.  Measured: 2-byte entries (8-byte blocks) 2
+        // blocks 417 ms, 3: 405, 4: 401 on 5,000 config-3 queries, one block
+        // 500; 4-byte entries (16-byte blocks) 1 block 1,841 ms, 2: 1,591, 4:
+        // 1,753 on 10,000 config-3 queries of the weighted t=5 kernel
         auto walk = [&]() {
-            constexpr int NB = 4;
+            constexpr int NB = E16 ? 4 : 2;
             const uint32_t end = beg + len;
             const uint32_t base = C16 ? slot & 0x7FFFFFFFu : slot, add = C16 ? 1u << ((slot >> 31) * 16u) : 0u;
             if (!RANGE) lane_hits += len;
@@ -606,7 +624,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
             for (int s = sub_lo + threadIdx.x; s < sub_lo + sub_n; s += Q_THREADS) {
                 unsigned long long *g = a.gcount + (row * a.S + s0 + s) * a.nlev;
                 for (int m = 0; m < a.nlev; m++) {
-                    const int64_t c = read_count<C16>(sm_acc, sm_log, nl, m, stride, s - sub_lo);
+                    const int64_t c = read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo);
                     if (c) atomicAdd(g + m, (unsigned long long)c);
                 }
             }
@@ -614,7 +632,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         for (int s = sub_lo + threadIdx.x; s < sub_lo + sub_n; s += Q_THREADS) {
             double k = 0.0;
             for (int m = 0; m < a.nlev; m++)
-                k += a.h[m] * (double)read_count<C16>(sm_acc, sm_log, nl, m, stride, s - sub_lo);
+                k += a.h[m] * (double)read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo);
             const int64_t sg = s0 + s;
             if (MODE == MODE_SCORE) {
                 const double kn = k * inv_dx * a.inv_ds[sg];
@@ -624,7 +642,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                 if (a.profile) {
                     uint64_t *pp = a.profile + (row * a.S + sg) * (a.l + 1);
                     for (int m = 0; m <= a.l; m++)
-                        pp[m] = m < a.nlev ? (uint64_t)read_count<C16>(sm_acc, sm_log, nl, m, stride, s - sub_lo) : 0;
+                        pp[m] = m < a.nlev ? (uint64_t)read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo) : 0;
                 }
             }
         }
@@ -727,6 +745,21 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
     ix->n_masks = n_masks;
     ix->acc_bytes = acc_bytes;
     ix->wide = spec->weighted ? 1 : 0;
+    ix->wmax = 1;
+    if (spec->weighted) {
+        // the largest window weight, from the device table (once per index)
+        uint8_t *h = (uint8_t *)malloc(spec->wd_len > 0 ? spec->wd_len : 1);
+        if (!h || cudaMemcpyAsync(h, spec->wd, spec->wd_len, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            free(h);
+            gkm_index_free(ix);
+            return gkm_fail(GKM_ERR_CUDA, "window weight table");
+        }
+        ix->wmax = 0;
+        for (int32_t k = 0; k < spec->wd_len; k++) ix->wmax = h[k] > ix->wmax ? h[k] : ix->wmax;
+        free(h);
+        if (ix->wmax == 0) ix->wmax = 1;
+    }
     int status = GKM_OK;
     uint32_t *ecount = nullptr, *base = nullptr, *keys = nullptr, *vals = nullptr, *kt = nullptr, *vt = nullptr;
     uint32_t total = 0;
@@ -824,7 +857,8 @@ extern "C" int gkm_index_status(gkm_index_t *ix, uint32_t *counts, int32_t wide,
                                         (cudaStream_t)stream);
         if (e != cudaSuccess) return gkm_cuda_status(e, "index status");
     }
-    if (wide >= 0) ix->wide = ix->spec.weighted ? 1 : wide;
+    // weighted: 32-bit counters, or 64-bit (2); unweighted: 16-bit (0) or 32-bit
+    if (wide >= 0) ix->wide = ix->spec.weighted ? (wide == 2 ? 2 : 1) : (wide ? 1 : 0);
     return GKM_OK;
 }
 
@@ -856,17 +890,18 @@ static QueryArgs query_args(const gkm_index_t *ix, const uint32_t *bx, const int
     a.n_lmers = ix->n_lmers;
     a.S = ix->S;
     a.tile_svs = ix->tile_svs;
-    a.sub_svs = ix->acc_bytes / (4 * ix->nlev);
+    a.sub_svs = ix->acc_bytes / ((ix->wide == 2 ? 8 : 4) * ix->nlev);
     a.status = ix->status;
     a.nlev = ix->nlev;
     a.dmax = ix->spec.dmax;
     for (int m = 0; m < 16; m++) a.h[m] = ix->spec.h[m];
     a.wd = ix->spec.wd;
     a.l = ix->spec.l;
+    a.wide_bound = (uint64_t)(ix->spec.include_rc ? 2 : 1) * (uint64_t)ix->W * ix->wmax * ix->wmax;
     return a;
 }
 
-template <bool WEIGHTED, int MODE, bool C16, bool E16>
+template <bool WEIGHTED, int MODE, bool C16, bool E16, bool C64 = false>
 static void launch_query(unsigned grid, size_t smem, cudaStream_t st, const QueryArgs &a)
 {
     // ids need a range test only for a self-Gram's diagonal or wide sub-ranges
@@ -875,9 +910,9 @@ static void launch_query(unsigned grid, size_t smem, cudaStream_t st, const Quer
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         index_query<WEIGHTED, MODE, C16, E16, false><<<grid, Q_THREADS, smem, st>>>(a);
     } else {
-        cudaFuncSetAttribute(index_query<WEIGHTED, MODE, C16, E16, true>,
+        cudaFuncSetAttribute(index_query<WEIGHTED, MODE, C16, E16, true, C64>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        index_query<WEIGHTED, MODE, C16, E16, true><<<grid, Q_THREADS, smem, st>>>(a);
+        index_query<WEIGHTED, MODE, C16, E16, true, C64><<<grid, Q_THREADS, smem, st>>>(a);
     }
 }
 
@@ -899,7 +934,9 @@ static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cu
     int64_t items = B * ix->tiles * a.nsplit;
     const int blocks = gkm_query_blocks();
     unsigned grid = (unsigned)(items < blocks ? items : blocks);
-    if (ix->spec.weighted)
+    if (ix->spec.weighted && ix->wide == 2)
+        launch_query<true, MODE, false, false, true>(grid, smem, st, q);
+    else if (ix->spec.weighted)
         launch_query<true, MODE, false, false>(grid, smem, st, q);
     else if (ix->ent16 && ix->wide)
         launch_query<false, MODE, false, true>(grid, smem, st, q);
@@ -1075,8 +1112,7 @@ extern "C" int gkm_index_score(const gkm_index_t *ix, const uint32_t *bx, const 
     }
     if (s == GKM_OK) {
         GKM_PREFER_SHARED(finish_scores);
-        GKM_PREFER_SHARED(finish_scores);
-    finish_scores<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(partial, B, ix->tiles, bias, scores);
+        finish_scores<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(partial, B, ix->tiles, bias, scores);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) s = gkm_cuda_status(e, "finish_scores");
     }

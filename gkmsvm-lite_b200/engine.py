@@ -239,21 +239,31 @@ class DeviceIndex:
         call("gkm_index_status", self.handle, ptr(buf), -1, _st())
         return buf
 
-    def set_wide(self, wide: bool) -> None:
-        call("gkm_index_status", self.handle, None, int(bool(wide)), _st())
+    def set_wide(self, wide: int) -> None:
+        """Counter width of later queries: unweighted 16-bit with the carry
+        log (0) or 32-bit (1); weighted 32-bit (0, 1) or 64-bit (2)."""
+        call("gkm_index_status", self.handle, None, int(wide), _st())
 
     def settle(self, before: torch.Tensor, rerun=None):
         """After a call bracketed by counters() snapshots: waits for the
         stream; if a query block's 16-bit carries outgrew its log anywhere in
         that window (this call's or a concurrent one's), reruns rerun() with
-        32-bit counters (exact either way).  A wrapped 32-bit count raises.
-        Returns True when it reran."""
+        32-bit counters, and if a weighted 32-bit count wrapped, with 64-bit
+        counters (exact either way).  A wrapped unweighted 32-bit count (past
+        2^32 matching window pairs of one row and one SV) raises.  Returns
+        True when it reran."""
         after = self.counters()
         torch.cuda.current_stream().synchronize()
         reran = False
-        if int(after[0]) != int(before[0]) and rerun is not None:
+        wide = 0
+        if rerun is not None:
+            if self.spec.c.weighted and int(after[1]) != int(before[1]):
+                wide = 2
+            elif int(after[0]) != int(before[0]):
+                wide = 1
+        if wide:
             reran = True
-            self.set_wide(True)
+            self.set_wide(wide)
             try:
                 b2 = self.counters()
                 rerun()
@@ -261,7 +271,7 @@ class DeviceIndex:
                 torch.cuda.current_stream().synchronize()
                 before = b2
             finally:
-                self.set_wide(False)
+                self.set_wide(0)
         if int(after[1]) != int(before[1]):
             raise _lib.GkmError(_lib.GKM_ERR_CAPACITY, "a weighted pair count passed 2^32 for one (row, SV) pair")
         return reran

@@ -124,9 +124,12 @@ int gkm_index_info(const gkm_index_t *index, int64_t *entries, int32_t *tiles,
  * into counts[2] (nullable; host or device memory): [0] query blocks whose
  * 16-bit counter carries outgrew their log, [1] 32-bit counters that wrapped.
  * The counts only grow: a call whose window (copy before, copy after, on its
- * stream) sees [0] change reruns with 32-bit counters; [1] changing is an
- * error.  wide >= 0 selects 32-bit counters (1) or 16-bit counters with the
- * carry log (0) for unweighted kernels. */
+ * stream) sees [0] change reruns with 32-bit counters; one that sees [1]
+ * change reruns with 64-bit counters (weighted kernels).  wide >= 0 selects,
+ * for unweighted kernels, 32-bit counters (1) or 16-bit counters with the
+ * carry log (0); for weighted kernels, 64-bit counters (2) or 32-bit (0, 1).
+ * Unweighted 32-bit counters wrap only past 2^32 matching window pairs of one
+ * (row, SV) pair; [1] moving there is an error. */
 int gkm_index_status(gkm_index_t *index, uint32_t *counts, int32_t wide, gkm_stream_t stream);
 
 /* K_raw [B, S] (nullable) and profiles [B, S, l+1] (nullable) through the

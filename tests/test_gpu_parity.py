@@ -432,6 +432,37 @@ def test_counter_carries_are_exact():
     np.testing.assert_allclose(got, want, rtol=RTOL, atol=ATOL)
 
 
+def test_weighted_counts_past_32_bits_are_exact():
+    """Window weights of 255 and poly-A rows push one (row, SV, level)
+    weighted count past 2^32 (the reference sums these in float64): the 32-bit
+    pass reports the wrap and the checked call reruns with 64-bit counters."""
+    rng = np.random.default_rng(9)
+    params = {"L": 11, "k": 7, "d": 3, "gamma": 1.0, "M": 255, "H": 1e6}
+    sv = np.concatenate([np.zeros((4, 1000), np.uint8), rng.integers(0, 4, (20, 1000)).astype(np.uint8)])
+    coef = rng.normal(size=24)
+    x = np.concatenate([np.zeros((1, 1000), np.uint8), rng.integers(0, 4, (2, 1000)).astype(np.uint8)])
+    kd = orc.KernelDef.from_params("wgkmrbf", params)
+    want_prof = orc.profiles(x, None, sv, None, kd)
+    assert want_prof[0, 0, 0] >= 2**32
+    m = gk.GkmSVM(sv, coef, 0.0, "wgkmrbf", params).cuda()
+    m.use_lmer_table = False
+    index = m._sv_index()
+    spec = m._spec()
+    # 300 rows: enough items that no row is split, each row whole in one block
+    xr = np.repeat(x, 100, axis=0)
+    fwd, rc, counts = engine.pack(spec, torch.from_numpy(xr).cuda(), None)
+    before = index.counters()
+    index.pairwise(fwd, counts, check=False)
+    after = index.counters()
+    torch.cuda.synchronize()
+    assert int(after[1]) > int(before[1])  # a 32-bit count wrapped
+    raw, prof = index.pairwise(fwd, counts, profile=True)
+    np.testing.assert_array_equal(_np(prof)[::100, :, :4].astype(np.uint64), want_prof[..., :4])
+    want = orc.scores(orc.OracleModel(sv, None, coef, 0.0, kd), x)
+    np.testing.assert_allclose(_np(m(xr))[::100], want, rtol=RTOL, atol=ATOL)
+    np.testing.assert_allclose(_np(m(x)), want, rtol=RTOL, atol=ATOL)
+
+
 @pytest.mark.parametrize("name", ["t2", "t3", "t4", "t5", "t6", "t0"])
 @pytest.mark.parametrize("graphs", [True, False])
 def test_batched_scorer_equals_model(small, name, graphs):
