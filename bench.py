@@ -125,11 +125,12 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip t=2, plain-call and CPU legs")
     ap.add_argument("--leg", default="all",
                     choices=["all", "gram", "train", "explain", "explain-pairs", "serve", "encode", "pairwise-forms",
-                             "weighted"],
+                             "weighted", "ism-index"],
                     help="gram / train / explain: run only the Gram-matrix, SMO training or config-4 ISM and "
                          "GkmExplain leg (one GPU), print its JSON")
     ap.add_argument("--gram-n", type=int, default=4000, help="sequences of the Gram-matrix leg")
     ap.add_argument("--weighted-n", type=int, default=20000, help="queries of the weighted (t=5) scoring leg")
+    ap.add_argument("--ism-rows", type=int, default=32, help="1,000 bp rows of the index-path ISM leg")
     return ap.parse_args()
 
 
@@ -1022,6 +1023,11 @@ def main():
         return 0
     if args.leg == "weighted":
         print(json.dumps(weighted_leg(args.weighted_n)), flush=True)
+        return 0
+    if args.leg == "ism-index":
+        import gkmsvm_lite_b200.synthetic as syn
+
+        print(json.dumps(ism_index_leg(*syn.config3_model(), rows=args.ism_rows)), flush=True)
         return 0
     if args.leg == "pairwise-forms":
         print(json.dumps(pairwise_forms_leg()), flush=True)

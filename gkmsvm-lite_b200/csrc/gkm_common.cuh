@@ -110,6 +110,8 @@ struct gkm_index {
     int64_t n_lmers;     // 4^l
     int64_t entries;     // indexed windows
     uint32_t *offsets;   // [tiles * n_lmers + 1] start of bucket (tile, v)
+    uint32_t *bwords;    // [tiles * n_lmers] (start - tile start) << lb | length (saturated); unweighted only
+    int32_t lb;          // length bits of a bucket word
     uint32_t *ent;       // [entries] local SV id (bits 0..23) | weight << 24 (weighted, or big tiles)
     uint16_t *ent16;     // [entries] local SV id (unweighted tiles of <= 65,536 SVs), else null
     uint32_t *masks;     // [n_masks] mask | level << 24
