@@ -41,9 +41,9 @@ WORKLOAD = ("config3: 72,000 SVs (200-500 bp, alpha ~ N(0, 0.1^2)), t=3 gkmrbf g
 
 # ncu on a 2,000-query launch of this workload (profiles/index_query_config3_t3_2000q.md):
 # throughput fractions of the units that bind the index query
-NCU_INDEX_QUERY = {"l1tex_data_pipe_frac": 0.928, "lts_throughput_frac": 0.315, "dram_bytes": 1.496e9,
-                   "shared_atomic_wavefronts_frac": 0.336, "global_load_wavefronts_frac": 0.313,
-                   "shared_atomic_bank_conflicts_per_wavefront": 0.60, "issue_active_frac": 0.654,
+NCU_INDEX_QUERY = {"l1tex_data_pipe_frac": 0.826, "lts_throughput_frac": 0.308, "dram_bytes": 1.485e9,
+                   "shared_atomic_wavefronts_frac": 0.352, "global_load_wavefronts_frac": 0.244,
+                   "shared_atomic_bank_conflicts_per_wavefront": 0.60, "issue_active_frac": 0.720,
                    "warps_active_frac": 0.50}
 
 
@@ -905,7 +905,8 @@ def run_b200(args):
                          "kernel": "index_query (fused SV-tile query + RBF + alpha reduce)",
                          "alg_bytes_per_launch": alg_bytes, "hits": hits, "lookups": lookups,
                          "frac_stored_entry_bytes": stored_bytes / (query_ms / 1e3) / 1e9 / peak,
-                         "binding_unit": "L1/shared atomics (the index is L2-resident: HBM is not what "
+                         "binding_unit": "the L1 data pipe (shared adds, bucket and entry gathers) and "
+                                         "instruction issue (the index is L2-resident: HBM is not what "
                                          "binds it)",
                          "ncu_small_case": NCU_INDEX_QUERY,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6.65 TB/s"},

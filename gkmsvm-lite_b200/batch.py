@@ -365,13 +365,18 @@ class _PerRowRunner:
 class BatchedIsm(_PerRowRunner):
     """gkmsvm_lite_b200.ism of device code batches through bucket graphs."""
 
-    def __init__(self, model):
+    def __init__(self, model, pass_positions: int = None):
+        """pass_positions: on the index path, at most this many positions per
+        pass (one short persistent query per pass, so that kernels of other
+        streams get the SMs between passes); None: as many as 1.5 GiB of
+        workspace holds."""
         super().__init__(model)
+        self.pass_positions = pass_positions
         self._work = None
         self._works = []  # every workspace a captured graph refers to
 
     def body(self, codes, lengths):
-        from .ism import _ism_rows, ism_workspace_bytes
+        from .ism import _ism_rows, ism_pass_bytes, ism_workspace_bytes
 
         m = self.model
         work = None
@@ -379,11 +384,13 @@ class BatchedIsm(_PerRowRunner):
             # the index path's workspace, shared by the buckets (their replays
             # are serial); grown for a bucket of more rows (the eager warm-up
             # allocates it, never the capture)
-            need = ism_workspace_bytes(m, codes.shape[0], codes.shape[1])
+            B, L = codes.shape
+            cap = None if self.pass_positions is None else ism_pass_bytes(m, B, self.pass_positions)
+            need = ism_workspace_bytes(m, B, L, cap)
             if self._work is None or self._work.numel() < need:
                 self._work = torch.empty(need, dtype=torch.uint8, device=codes.device)
                 self._works.append(self._work)
-            work = self._work
+            work = self._work[:need]  # the call sizes its passes by the bytes it is given
         return _ism_rows(m, codes, lengths, codes.device, check=False, work=work)
 
 

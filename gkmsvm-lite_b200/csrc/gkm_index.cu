@@ -309,6 +309,7 @@ struct QueryArgs {
     // SV's windows x the largest weight product); an item whose windows times
     // this stays below 2^32 cannot wrap a counter, and adds without checking
     uint64_t wide_bound;
+    int skip_empty;       // rows without windows write nothing (their outputs are never read)
     int nsplit;           // items per (row, tile): window ranges of split_w windows
     int split_w;
     unsigned long long *gcount;  // MODE_COUNT: [B, S, nlev] summed counts
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
     const int n = a.cx[row];
     // this item's windows [i0, i1) of the row (the whole row unless split)
     const int i0 = min(n, ks * a.split_w), i1 = min(n, i0 + a.split_w);
-    if (MODE == MODE_COUNT && i0 >= i1) continue;
+    if ((MODE == MODE_COUNT || a.skip_empty) && i0 >= i1) continue;
     const uint32_t *x = a.bx + row * a.W;
     const uint32_t *off = a.off + (int64_t)t * a.n_lmers;
     const uint32_t *bw = WEIGHTED ? nullptr : a.bw + (int64_t)t * a.n_lmers;
@@ -561,9 +562,13 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                         en[4 * k + 3] = w[k].w;
                     }
                 }
+                // the iteration's slots inside [beg, end) as one bit mask
+                const uint32_t lo = beg > e ? min(beg - e, 4u * NB) : 0u;
+                const uint32_t hi = end > e ? min(end - e, 4u * NB) : 0u;
+                const uint32_t valid = hi > lo ? ((1u << hi) - 1u) ^ ((1u << lo) - 1u) : 0u;
 #pragma unroll
                 for (int q = 0; q < 4 * NB; q++)
-                    if (e + q >= beg && e + q < end) count_hit(en[q], base, add);
+                    if (valid & (1u << q)) count_hit(en[q], base, add);
             }
         };
         if (nwin >= Q_WARPS) {
@@ -1015,11 +1020,17 @@ static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cu
 // kept within 256 MB.  1: no split.
 static int split_plan(const gkm_index_t *ix, int64_t B, int64_t W)
 {
-    const int64_t items = B * ix->tiles, target = 2LL * gkm_query_blocks();
-    if (items >= target || W < 64) return 1;
+#ifndef GKM_SPLIT_W
+#define GKM_SPLIT_W 32
+#endif
+#ifndef GKM_SPLIT_T
+#define GKM_SPLIT_T 2
+#endif
+    const int64_t items = B * ix->tiles, target = GKM_SPLIT_T * (int64_t)gkm_query_blocks();
+    if (items >= target || W < 2 * GKM_SPLIT_W) return 1;
     if (B * ix->S * ix->nlev * 8 > (256LL << 20)) return 1;
     int64_t ns = (target + items - 1) / items;
-    if (ns > W / 32) ns = W / 32;
+    if (ns > W / GKM_SPLIT_W) ns = W / GKM_SPLIT_W;
     return ns < 2 ? 1 : (int)ns;
 }
 
@@ -1340,14 +1351,34 @@ __global__ void ism_index_finish(const double *__restrict__ kbuf, int64_t S, con
     if (threadIdx.x == 0) out[(b * 4 + xp) * L + p] = 0.0;
 }
 
+// Reference scores of the rows, sum_s coef_s f(ref[b, s] inv_dx[b] inv_ds[s]),
+// with ism_index_finish's arithmetic and reduction order (256 threads, s
+// strided), so that a mutant's delta is the difference of two sums taken alike
+__global__ void ism_ref_score(const double *__restrict__ ref, int64_t S, const double *__restrict__ inv_dx,
+                              const double *__restrict__ inv_ds, const double *__restrict__ coef, double gamma,
+                              int rbf, double *__restrict__ out)
+{
+    __shared__ double red[32];
+    const int64_t b = blockIdx.x;
+    const double z = inv_dx[b];
+    double acc = 0.0;
+    for (int64_t s = threadIdx.x; s < S; s += blockDim.x) {
+        const double kn = ref[b * S + s] * z * inv_ds[s];
+        acc += coef[s] * (rbf ? exp(gamma * (kn - 1.0)) : kn);
+    }
+    acc = gkm_block_sum(acc, red);
+    if (threadIdx.x == 0) out[b] = acc;
+}
+
 static size_t ism_align(size_t n) { return (n + 255) & ~(size_t)255; }
 
-// workspace bytes of a chunk: query rows (l slots), their counts and slot
-// weights, and their K_raw rows
+// workspace bytes of a chunk: the rows' reference scores, query rows (l
+// slots), their counts and slot weights, and their K_raw rows
 static size_t ism_chunk_bytes(const gkm_index_t *ix, const IsmChunk &ck)
 {
     const size_t rows = (size_t)ck.rows(), l = (size_t)ix->spec.l;
-    return ism_align(rows * l * 4) + ism_align(rows * 4) + ism_align(rows * l) + rows * (size_t)ix->S * 8;
+    return ism_align((size_t)ck.B * 8) + ism_align(rows * l * 4) + ism_align(rows * 4) + ism_align(rows * l) +
+           rows * (size_t)ix->S * 8;
 }
 
 extern "C" int gkm_index_mutants_workspace(const gkm_index_t *ix, int64_t B, int64_t L, int64_t *min_bytes,
@@ -1366,9 +1397,9 @@ extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, con
                                  const double *coef, double gamma, int32_t rbf, double *out, void *workspace,
                                  int64_t workspace_bytes, gkm_stream_t stream)
 {
-    (void)inv_dx;
-    if (!ix || !fwd || !counts || !ref_raw || !ref_score || !inv_dmut || !inv_ds || !coef || !out)
+    if (!ix || !fwd || !counts || !ref_raw || !inv_dmut || !inv_ds || !coef || !out)
         return gkm_fail(GKM_ERR_INVALID, "null argument");
+    if (!ref_score && !inv_dx) return gkm_fail(GKM_ERR_INVALID, "reference scores need inv_dx");
     if (B < 0 || L < 0 || W < 0) return gkm_fail(GKM_ERR_INVALID, "negative size");
     if (B == 0 || L == 0) return GKM_OK;
     if (!workspace || ((uintptr_t)workspace & 255))
@@ -1390,12 +1421,21 @@ extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, con
     if (np == 0)
         return gkm_fail(GKM_ERR_CAPACITY, "ISM workspace of %lld bytes holds no position (needs %lld)",
                         (long long)workspace_bytes, (long long)ism_chunk_bytes(ix, IsmChunk{1, B, l}));
+    double *rscore = (double *)workspace;  // the first bytes of the workspace
+    if (ref_score) {
+        cudaError_t e = cudaMemcpyAsync(rscore, ref_score, sizeof(double) * B, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return gkm_cuda_status(e, "ISM reference scores");
+    } else {
+        GKM_PREFER_SHARED(ism_ref_score);
+        ism_ref_score<<<(unsigned)B, 256, 0, st>>>(ref_raw, S, inv_dx, inv_ds, coef, gamma, rbf, rscore);
+        GKM_CHECK_LAUNCH("ism_ref_score");
+    }
     for (int64_t p0 = 0; p0 < L; p0 += np) {
         const int64_t n_p = min(np, L - p0);
         const IsmChunk ck{n_p, B, n_p + l - 1};
         const int64_t rows = ck.rows();
         if (rows > 0x7FFFFFFFLL) return gkm_fail(GKM_ERR_UNSUPPORTED, "too many ISM rows in one chunk");
-        uint8_t *w = (uint8_t *)workspace;
+        uint8_t *w = (uint8_t *)workspace + ism_align((size_t)B * 8);
         uint32_t *qrows = (uint32_t *)w;
         w += ism_align((size_t)rows * l * 4);
         int32_t *qcnt = (int32_t *)w;
@@ -1410,10 +1450,13 @@ extern "C" int gkm_index_mutants(const gkm_index_t *ix, const uint32_t *fwd, con
         QueryArgs a = query_args(ix, qrows, qcnt, l);
         a.wq = ix->spec.weighted ? qwt : nullptr;
         a.raw = kbuf;
+        // query rows with no window (positions past a row's end, rows of
+        // length 0 padding a batch) are never read by ism_index_finish
+        a.skip_empty = 1;
         GKM_TRY(query_launch<MODE_RAW>(ix, a, rows, st));
         GKM_PREFER_SHARED(ism_index_finish);
         ism_index_finish<<<(unsigned)(n_p * B), 256, 0, st>>>(kbuf, S, fwd, counts, W, L, l, p0, ck, ref_raw,
-                                                             ref_score, inv_dmut, inv_ds, coef, gamma, rbf, out);
+                                                             rscore, inv_dmut, inv_ds, coef, gamma, rbf, out);
         GKM_CHECK_LAUNCH("ism_index_finish");
     }
     return GKM_OK;

@@ -89,10 +89,9 @@ def _ism_index(model, fwd, rc, counts, L, check=True, work=None):
         work = ism_workspace(model, B, L, fwd.device)
 
     def run():
+        # the reference rows' K_raw; their scores come from it inside the call
         ref_raw, _ = index.pairwise(fwd, counts, check=False)
-        ref_score = index.score(fwd, counts, inv_dx, model._inv_ds(), model._sv_coef(), gamma, rbf, 0.0,
-                                check=False)
-        call("gkm_index_mutants", index.handle, ptr(fwd), ptr(counts), B, W, L, ptr(ref_raw), ptr(ref_score),
+        call("gkm_index_mutants", index.handle, ptr(fwd), ptr(counts), B, W, L, ptr(ref_raw), None,
              ptr(inv_dx), ptr(inv_dmut), ptr(model._inv_ds()), ptr(model._sv_coef()), float(gamma), int(rbf),
              ptr(out), ptr(work), int(work.numel()), stream_handle())
         return out
@@ -107,6 +106,15 @@ def ism_workspace_bytes(model, B: int, L: int, cap: int = None) -> int:
     lo, hi = ctypes.c_int64(), ctypes.c_int64()
     call("gkm_index_mutants_workspace", model._sv_index().handle, B, L, ctypes.byref(lo), ctypes.byref(hi))
     return max(lo.value, min(hi.value, _WORKSPACE_BYTES if cap is None else cap))
+
+
+def ism_pass_bytes(model, B: int, positions: int) -> int:
+    """Workspace bytes of an index-path ISM pass over `positions` positions of
+    B rows (a workspace of this size makes every pass that short)."""
+    lo, hi = ctypes.c_int64(), ctypes.c_int64()
+    call("gkm_index_mutants_workspace", model._sv_index().handle, B, max(1, int(positions)), ctypes.byref(lo),
+         ctypes.byref(hi))
+    return hi.value
 
 
 def ism_workspace(model, B: int, L: int, device, cap: int = None) -> torch.Tensor:

@@ -65,12 +65,17 @@ class GkmServer:
 
     def __init__(self, backend, *, max_batch_rows: int = 8192, max_inflight: int = 2,
                  memory_reserve: int = 2 << 30, max_wait_s: float = 0.002, max_side_rows: int = 4,
-                 side_yield_s: float = 0.05):
+                 side_yield_s: float = 0.0):
         """side_yield_s > 0: before each ISM / GkmExplain call the side worker
         waits (at most this long) until no scoring pass is in flight or
         waiting, so the two kinds of work share the GPU in time: a scoring
         pass's index-query blocks take a whole SM's shared memory and can sit
-        behind a side call's kernels until they finish."""
+        behind a side call's kernels until they finish.  Off by default: the
+        GPU backend cuts ISM into short passes on a low-priority stream, so a
+        scoring pass waits for one pass at most, and waiting before every side
+        call starved side work whenever scoring stayed busy (measured, config-5
+        mix at 50 % load: worst p99 over six runs 919 ms with a 50 ms yield,
+        275 ms without)."""
         self.backend = backend
         self.max_batch_rows = max_batch_rows
         self.max_inflight = max_inflight
@@ -289,11 +294,15 @@ class GpuBackend:
     # the index query then splits their long rows over the whole GPU
     direct_rows = 64
 
-    def __init__(self, model, slots: int = 2, side_sm_share: float = 1.0, side_graphs: bool = True):
+    def __init__(self, model, slots: int = 2, side_sm_share: float = 1.0, side_graphs: bool = True,
+                 side_pass_positions: int = 128):
         """side_sm_share: the share of the SMs the side worker's persistent
         index queries may take (1: all), so that a scoring pass launched
         meanwhile finds SMs free; side_graphs: ISM / GkmExplain through the
-        bucketed graph runners (else direct ism() / gkmexplain() calls)."""
+        bucketed graph runners (else direct ism() / gkmexplain() calls);
+        side_pass_positions: index-path ISM passes of at most this many
+        positions (None: as many as the workspace holds), so that a scoring
+        pass waits for at most one short side kernel."""
         import torch
 
         from .batch import BatchedScorer, DirectScorer
@@ -313,6 +322,7 @@ class GpuBackend:
         props = torch.cuda.get_device_properties(model._device)
         self.side_blocks = 0 if side_sm_share >= 1 else max(1, int(props.multi_processor_count * side_sm_share))
         self.side_graphs = side_graphs
+        self.side_pass_positions = side_pass_positions
         # ISM / GkmExplain in bucket-shaped CUDA graphs, one runner per kind
         # (and explain mode), built by the side worker thread
         self.side_runners: dict = {}
@@ -344,8 +354,8 @@ class GpuBackend:
             for key in ["ism"] + [("explain", m) for m in explain_modes]:
                 runner = self.side_runners.get(key)
                 if runner is None:
-                    runner = self.side_runners[key] = (BatchedIsm(self.model) if key == "ism"
-                                                       else BatchedExplain(self.model, key[1]))
+                    runner = self.side_runners[key] = (BatchedIsm(self.model, self.side_pass_positions)
+                                                       if key == "ism" else BatchedExplain(self.model, key[1]))
                 try:
                     for L in lengths:
                         x = torch.zeros((runner.row_granule, L), dtype=torch.uint8, device=dev)
@@ -481,7 +491,8 @@ class GpuBackend:
                 runner = ((lambda x, ln: ism_call(self.model, x, lengths=ln)) if key == "ism" else
                           (lambda x, ln, mode=reqs[0].mode: gkmexplain(self.model, x, lengths=ln, mode=mode)))
             else:
-                runner = BatchedIsm(self.model) if key == "ism" else BatchedExplain(self.model, reqs[0].mode)
+                runner = (BatchedIsm(self.model, self.side_pass_positions) if key == "ism"
+                          else BatchedExplain(self.model, reqs[0].mode))
             self.side_runners[key] = runner
         with torch.cuda.stream(self.side_stream):
             if self.side_graphs:

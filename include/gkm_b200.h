@@ -229,8 +229,10 @@ int gkm_ism_table(const gkm_spec *spec, const double *table, const uint32_t *fwd
  * Allocates nothing: workspace (256-byte aligned, workspace_bytes) holds the
  * query rows and K_raw rows of as many positions per pass as fit; it must
  * hold at least gkm_index_mutants_workspace's min_bytes (GKM_ERR_CAPACITY
- * otherwise); all_bytes does every position in one pass.  inv_dx is unused
- * (kept for the operator's argument list).
+ * otherwise); all_bytes does every position in one pass.  ref_score [B]
+ * (nullable): the rows' scores without bias; null computes them from ref_raw
+ * and inv_dx with the arithmetic of the mutants' sums (one pass over ref_raw
+ * instead of another index query).
  * Replaces LmerIndex.mutants (kernels/lmer_index.py:326-374,
  * kernels/lmer_index_cpu.py:203-285). */
 int gkm_index_mutants_workspace(const gkm_index_t *index, int64_t B, int64_t L, int64_t *min_bytes,
