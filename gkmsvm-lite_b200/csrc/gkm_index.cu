@@ -10,6 +10,8 @@
 #include <stdint.h>
 #include <stdlib.h>
 
+#include <type_traits>
+
 #include "gkm_common.cuh"
 
 namespace {
@@ -447,6 +449,17 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
     const double inv_dx = MODE == MODE_SCORE ? a.inv_dx[row] : 0.0;
     double part = 0.0;
     const int sub = C16 ? ns : a.sub_svs;
+    if (MODE == MODE_SCORE && i0 >= i1) {
+        // a row without windows (rows of length 0 pad a batch to its graph
+        // bucket): every K(row, s) is 0, so each SV's term is coef f(0), with
+        // the arithmetic and order of a one-pass flush below -- no counters to
+        // clear, no walk
+        for (int s = threadIdx.x; s < ns; s += Q_THREADS) {
+            const int64_t sg = s0 + s;
+            const double kn = 0.0 * inv_dx * a.inv_ds[sg];
+            part += a.coef[sg] * (a.rbf ? exp(a.gamma * (kn - 1.0)) : kn);
+        }
+    } else
     for (int sub_lo = 0; sub_lo < ns; sub_lo += sub) {
         const int sub_n = min(sub, ns - sub_lo);
         const int stride = C16 ? St : sub_n;
@@ -497,12 +510,15 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         // slot, and the query window's weight
         uint32_t wq = 1, beg = 0, len = 0, slot = 0;
         // one index entry en of this lane's bucket: counter word base + id
-        // (C16: add `add` to it, the level's 16-bit field; wide: row base)
-        auto count_hit = [&](uint32_t en, uint32_t base, uint32_t add) {
+        // (C16: add `add` to it, the level's 16-bit field; wide: row base).
+        // PLAIN (a compile-time flag of the counting loops): C16 plain adds
+        // (not the carry-logged retry), wide adds that cannot wrap
+        auto count_hit = [&](auto PLAIN, uint32_t en, uint32_t base, uint32_t add) {
+            constexpr bool plain = decltype(PLAIN)::value;
             const uint32_t id = E16 ? en : (en & 0x00FFFFFFu);
             if (RANGE && (id < id_lo || id >= id_hi)) return;
             if (C16) {
-                if (logged) {
+                if (!plain) {
                     count16(sm_acc, base + id, add, add * 0xFFFFu, &nlog, sm_log, a.status);
                 } else {
                     atomicAdd(sm_acc + base + id, add);
@@ -513,7 +529,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                           (unsigned long long)(WEIGHTED ? wq * (en >> 24) : 1u));
             } else {
                 const uint32_t inc = WEIGHTED ? wq * (en >> 24) : 1u;
-                if (wide_safe) {
+                if (plain) {
                     atomicAdd(sm_acc + base + id, inc);
                 } else {
                     const uint32_t old = atomicAdd(sm_acc + base + id, inc);
@@ -528,7 +544,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         // blocks 417 ms, 3: 405, 4: 401 on 5,000 config-3 queries, one block
         // 500; 4-byte entries (16-byte blocks) 1 block 1,841 ms, 2: 1,591, 4:
         // 1,753 on 10,000 config-3 queries of the weighted t=5 kernel
-        auto walk = [&]() {
+        auto walk = [&](auto PLAIN) {
             constexpr int NB = E16 ? 4 : 2;
             const uint32_t end = beg + len;
             const uint32_t base = C16 ? slot & 0x7FFFFFFFu : slot, add = C16 ? 1u << ((slot >> 31) * 16u) : 0u;
@@ -568,63 +584,70 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                 const uint32_t valid = hi > lo ? ((1u << hi) - 1u) ^ ((1u << lo) - 1u) : 0u;
 #pragma unroll
                 for (int q = 0; q < 4 * NB; q++)
-                    if (valid & (1u << q)) count_hit(en[q], base, add);
+                    if (valid & (1u << q)) count_hit(PLAIN, en[q], base, add);
             }
         };
-        if (nwin >= Q_WARPS) {
-            // the row's windows to the warps in turn, all masks of a window in
-            // one warp
-            for (int i = i0 + warp; i < i1; i += Q_WARPS) {
-                const uint32_t u = x[i];
-                wq = window_weight(i);
-                lane_mask(u, lane, beg, len, slot);
-                for (int c0 = 0; c0 < n_masks; c0 += 32) {
-                    // the next chunk's buckets, loaded while this one is counted
-                    uint32_t nbeg, nlen, nslot;
-                    lane_mask(u, c0 + 32 + lane, nbeg, nlen, nslot);
-                    walk();
-                    beg = nbeg;
-                    len = nlen;
-                    slot = nslot;
-                }
-            }
-        } else {
-            // rows of fewer windows than warps (ISM window sets, the ends of
-            // row splits): (window, chunk of 32 masks) units, window-major, in
-            // one contiguous range per warp, so every warp has work
-            const int64_t nunit = (int64_t)nwin * nchunk;
-            const int64_t ub = nunit * warp / Q_WARPS, ue = nunit * (warp + 1) / Q_WARPS;
-            if (ub < ue) {
-                int win = (int)(ub / nchunk), ch = (int)(ub - (int64_t)win * nchunk);
-                uint32_t u = x[i0 + win];
-                wq = window_weight(i0 + win);
-                lane_mask(u, ch * 32 + lane, beg, len, slot);
-                for (int64_t un = ub; un < ue; un++) {
-                    // the next unit's window and buckets, loaded while this one is counted
-                    int nw = win, nc = ch + 1;
-                    if (nc == nchunk) {
-                        nw = win + 1;
-                        nc = 0;
+        // the item's windows to the warps, counted in one of two compiled forms
+        auto count_item = [&](auto PLAIN) {
+            if (nwin >= Q_WARPS) {
+                // the row's windows to the warps in turn, all masks of a window in
+                // one warp
+                for (int i = i0 + warp; i < i1; i += Q_WARPS) {
+                    const uint32_t u = x[i];
+                    wq = window_weight(i);
+                    lane_mask(u, lane, beg, len, slot);
+                    for (int c0 = 0; c0 < n_masks; c0 += 32) {
+                        // the next chunk's buckets, loaded while this one is counted
+                        uint32_t nbeg, nlen, nslot;
+                        lane_mask(u, c0 + 32 + lane, nbeg, nlen, nslot);
+                        walk(PLAIN);
+                        beg = nbeg;
+                        len = nlen;
+                        slot = nslot;
                     }
-                    uint32_t nu = u, nwq = wq, nbeg = 0, nlen = 0, nslot = 0;
-                    if (un + 1 < ue) {
-                        if (nw != win) {
-                            nu = x[i0 + nw];
-                            nwq = window_weight(i0 + nw);
+                }
+            } else {
+                // rows of fewer windows than warps (ISM window sets, the ends of
+                // row splits): (window, chunk of 32 masks) units, window-major, in
+                // one contiguous range per warp, so every warp has work
+                const int64_t nunit = (int64_t)nwin * nchunk;
+                const int64_t ub = nunit * warp / Q_WARPS, ue = nunit * (warp + 1) / Q_WARPS;
+                if (ub < ue) {
+                    int win = (int)(ub / nchunk), ch = (int)(ub - (int64_t)win * nchunk);
+                    uint32_t u = x[i0 + win];
+                    wq = window_weight(i0 + win);
+                    lane_mask(u, ch * 32 + lane, beg, len, slot);
+                    for (int64_t un = ub; un < ue; un++) {
+                        // the next unit's window and buckets, loaded while this one is counted
+                        int nw = win, nc = ch + 1;
+                        if (nc == nchunk) {
+                            nw = win + 1;
+                            nc = 0;
                         }
-                        lane_mask(nu, nc * 32 + lane, nbeg, nlen, nslot);
+                        uint32_t nu = u, nwq = wq, nbeg = 0, nlen = 0, nslot = 0;
+                        if (un + 1 < ue) {
+                            if (nw != win) {
+                                nu = x[i0 + nw];
+                                nwq = window_weight(i0 + nw);
+                            }
+                            lane_mask(nu, nc * 32 + lane, nbeg, nlen, nslot);
+                        }
+                        walk(PLAIN);
+                        beg = nbeg;
+                        len = nlen;
+                        slot = nslot;
+                        win = nw;
+                        ch = nc;
+                        u = nu;
+                        wq = nwq;
                     }
-                    walk();
-                    beg = nbeg;
-                    len = nlen;
-                    slot = nslot;
-                    win = nw;
-                    ch = nc;
-                    u = nu;
-                    wq = nwq;
                 }
             }
-        }
+        };
+        if (C16 ? !logged : wide_safe)
+            count_item(std::true_type{});
+        else
+            count_item(std::false_type{});
         __syncthreads();
         if (!C16 || logged) break;
         {
@@ -1020,17 +1043,14 @@ static int query_launch(const gkm_index_t *ix, const QueryArgs &a, int64_t B, cu
 // kept within 256 MB.  1: no split.
 static int split_plan(const gkm_index_t *ix, int64_t B, int64_t W)
 {
-#ifndef GKM_SPLIT_W
-#define GKM_SPLIT_W 32
-#endif
-#ifndef GKM_SPLIT_T
-#define GKM_SPLIT_T 2
-#endif
-    const int64_t items = B * ix->tiles, target = GKM_SPLIT_T * (int64_t)gkm_query_blocks();
-    if (items >= target || W < 2 * GKM_SPLIT_W) return 1;
+    // (measured on 1..64 rows of 300..2,000 bp, t=3 and t=5 on 72,000 SVs:
+    // ranges of at least 64, 96 or 160 windows, or one item per block, were
+    // as fast or slower)
+    const int64_t items = B * ix->tiles, target = 2LL * gkm_query_blocks();
+    if (items >= target || W < 64) return 1;
     if (B * ix->S * ix->nlev * 8 > (256LL << 20)) return 1;
     int64_t ns = (target + items - 1) / items;
-    if (ns > W / GKM_SPLIT_W) ns = W / GKM_SPLIT_W;
+    if (ns > W / 32) ns = W / 32;
     return ns < 2 ? 1 : (int)ns;
 }
 
