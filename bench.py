@@ -41,9 +41,9 @@ WORKLOAD = ("config3: 72,000 SVs (200-500 bp, alpha ~ N(0, 0.1^2)), t=3 gkmrbf g
 
 # ncu on a 2,000-query launch of this workload (profiles/index_query_config3_t3_2000q.md):
 # throughput fractions of the units that bind the index query
-NCU_INDEX_QUERY = {"l1tex_data_pipe_frac": 0.826, "lts_throughput_frac": 0.308, "dram_bytes": 1.485e9,
-                   "shared_atomic_wavefronts_frac": 0.352, "global_load_wavefronts_frac": 0.244,
-                   "shared_atomic_bank_conflicts_per_wavefront": 0.60, "issue_active_frac": 0.720,
+NCU_INDEX_QUERY = {"l1tex_data_pipe_frac": 0.862, "lts_throughput_frac": 0.344, "dram_bytes": 1.503e9,
+                   "shared_atomic_wavefronts_frac": 0.375, "global_load_wavefronts_frac": 0.266,
+                   "shared_atomic_bank_conflicts_per_wavefront": 0.60, "issue_active_frac": 0.671,
                    "warps_active_frac": 0.50}
 
 

@@ -607,7 +607,10 @@ class IndexBaseline:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().orc_index_free(self.h)
+            try:
+                lib().orc_index_free(self.h)
+            except TypeError:  # interpreter shutdown: the module's globals are gone
+                pass
             self.h = None
 
     def scores(self, xc, xl=None, threads: int = 1, diag_x=None) -> np.ndarray:

@@ -494,6 +494,37 @@ def test_batched_scorer_config1_table_and_index():
             np.testing.assert_allclose(_np(bs.score(x)), want, rtol=RTOL, atol=ATOL)
 
 
+def test_bucket_words_of_large_tiles():
+    """48,000 SVs of 500 bp: each of the two SV tiles holds ~23.5M index
+    entries, more than 24 bits of bucket begin, so the bucket words keep 7 bits
+    of length (a bucket of 127 or more entries reads its end from the offsets).
+    Profiles bit-exact to the all-pairs forms, scores equal to the oracle's."""
+    import gkmsvm_lite_b200.synthetic as syn
+
+    rng = np.random.default_rng(41)
+    n_sv = 48000
+    sv = syn.random_codes(rng, n_sv, 500)
+    sv[:3] = 0  # poly-A SVs: one bucket of ~1,500 entries per tile
+    coef = rng.normal(0, 0.1, n_sv)
+    xl = np.array([500, 320, 75, 11])
+    x = syn.ragged_codes(rng, xl)
+    x[0, 100:200] = 0
+    params = {"L": 11, "k": 7, "d": 3, "gamma": 2.0}
+    m = gk.GkmSVM(sv, coef, 0.0, "gkmrbf", params).cuda()
+    m.use_lmer_table = False
+    index = m._sv_index()
+    assert index.tiles == 2 and index.entries / index.tiles > 2**24
+    spec = m._spec()
+    fwd, rc, counts = engine.pack(spec, torch.from_numpy(x).cuda(), xl)
+    _, p_index = index.pairwise(fwd, counts, raw=False, profile=True)
+    by, ry, cy = m._sv_packed()
+    _, p = engine.pairwise(spec, fwd, counts, by, ry, cy, raw=False, profile=True, method="dense")
+    assert torch.equal(p, p_index)
+    kd = orc.KernelDef.from_params("gkmrbf", params)
+    want = orc.IndexBaseline(orc.OracleModel(sv, None, coef, 0.0, kd), threads=8).scores(x, xl, threads=8)
+    np.testing.assert_allclose(_np(m(x, lengths=xl)).ravel(), want.ravel(), rtol=RTOL, atol=ATOL)
+
+
 def test_large_neighbourhood_index_past_reference_limit():
     """t=0 gkm_cnt l=11 k=7 with no d (31,714 neighbour masks, read from global
     memory) on 1,500 SVs: the index serves it (its measured cost is below the
