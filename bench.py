@@ -50,7 +50,7 @@ NCU_INDEX_QUERY = {"l1tex_data_pipe_frac": 0.862, "lts_throughput_frac": 0.344, 
 def job_config(queries: int, world: int) -> dict:
     """The workload description both arms print (the same dict for both)."""
     return {"workload": WORKLOAD, "queries_per_rank": queries, "svs": 72000, "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (100k packed queries: 1.6 GB; the 148 MB SV index also exceeds the 126 MB L2)"}
+            "l2": "inputs larger than L2 (100k packed queries: 1.6 GB; the 165 MB SV index with its bucket words also exceeds the 126 MB L2)"}
 
 
 def shard_seed(rank: int, base: int = 102) -> int:

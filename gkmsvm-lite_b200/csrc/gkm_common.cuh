@@ -119,6 +119,8 @@ struct gkm_index {
     int64_t bytes;
     int32_t acc_bytes;   // shared memory left for counters in a query block
     int32_t wide;        // 1: 32-bit counters (weighted, or after a carry-log overflow)
+    int32_t packed;      // narrow counters: 1 every level of an SV in one word, 0 two levels per word
+    uint32_t pack_w[8];  // packed: bits of each level's field
     uint32_t wmax;       // largest window weight (1 unweighted)
     unsigned int *status; // [2] query event counts (see gkm_index_status)
     unsigned int *queues;            // [GKM_QUEUE_SLOTS] work-queue heads, one per call in flight

@@ -273,13 +273,40 @@ __global__ void bucket_words(const uint32_t *__restrict__ off, int64_t nbuckets,
 
 constexpr int Q_THREADS = 1024;
 constexpr int Q_WARPS = Q_THREADS / 32;
-constexpr int LOG_CAP = 64;            // carry events a block can log (16-bit counters)
+constexpr int LOG_CAP = 64;            // carry events a block can log (narrow counters)
 constexpr int MASKS_SMEM_MAX = 6144;   // neighbour masks staged in shared memory up to this
 // MODE_COUNT: an item covers a range of a row's windows (a row split) and adds
 // its exact per-(SV, level) counts into gcount; a finish kernel turns the
 // summed counts into K_raw, profiles or scores.
 enum { MODE_SCORE = 0, MODE_RAW = 1, MODE_COUNT = 2 };
-enum { EV_LOWCARRY = 0, EV_WRAP = 1 };
+
+// Narrow (C16) counters: 32-bit words split into fields, one level of one SV
+// per field.  Paired layout: two 16-bit fields per word, levels 2j and 2j+1 of
+// an SV in word j * tile_svs + s.  Packed layout (unweighted, <= 4 levels):
+// every level of SV s in word s, field m at bit shift(m) and width(m), so a
+// tile holds twice the SVs.  Field g of a layout: shift (fsh >> 5g) & 31,
+// width (fw >> 5g) & 31; nf fields per word.
+struct Narrow {
+    int packed, nf;
+    uint32_t fsh, fw;
+    __device__ __forceinline__ uint32_t shift(int g) const { return (fsh >> (5 * g)) & 31u; }
+    __device__ __forceinline__ uint32_t mask(int g) const
+    {
+        const uint32_t w = (fw >> (5 * g)) & 31u;
+        return w ? (1u << w) - 1u : 0xFFFFFFFFu;  // width 0 stands for 32
+    }
+    __device__ __forceinline__ uint32_t width(int g) const
+    {
+        const uint32_t w = (fw >> (5 * g)) & 31u;
+        return w ? w : 32u;
+    }
+    // counter word and field of level m of local SV s
+    __device__ __forceinline__ uint32_t word(int m, int St, int s) const
+    {
+        return packed ? (uint32_t)s : (uint32_t)((m >> 1) * St + s);
+    }
+    __device__ __forceinline__ int field(int m) const { return packed ? m : (m & 1); }
+};
 
 struct QueryArgs {
     const uint32_t *bx;
@@ -301,6 +328,7 @@ struct QueryArgs {
     int nlev;
     int dmax;
     double h[16];
+    Narrow nw;            // narrow counters' layout
     const uint8_t *wd;
     const uint8_t *wq;    // [rows, W] query window weights (null: from the row's count)
     unsigned int *status; // [2] event counts: a block's carry log overflowed, a wide counter wrapped
@@ -337,48 +365,49 @@ __host__ __device__ inline size_t query_fixed_smem(int n_masks)
     return m + LOG_CAP * 4 + 64;
 }
 
-// C16: unweighted pair counts in 16-bit fields, two SVs of one level per
-// 32-bit word.  A field that passes 65535 carries into its neighbour (or out
-// of the word); the adder sees that in the value atomicAdd returns and logs
-// it, and the epilogue adds the carries back, so the counts stay exact.
+// C16: unweighted pair counts in narrow fields (Narrow).  A field that passes
+// its largest value carries into the next field (or out of the word); the
+// carry-logged adder sees that in the value atomicAdd returns and logs it, and
+// the epilogue adds the carries back, so the counts stay exact.
 template <bool C16, bool C64>
 __device__ __forceinline__ int64_t read_count(const uint32_t *acc, const uint32_t *log, int nlog, int m, int St,
-                                              int s)
+                                              int s, const Narrow &nw)
 {
     if (C64) return (int64_t)((const unsigned long long *)acc)[m * St + s];
     if (!C16) return acc[m * St + s];
-    // levels 2j and 2j+1 of SV s share word j * St + s (low and high half)
-    const uint32_t word = (uint32_t)((m >> 1) * St + s), half = (uint32_t)(m & 1);
-    int64_t f = (acc[word] >> (16 * half)) & 0xFFFFu;
+    const uint32_t word = nw.word(m, St, s);
+    const int g = nw.field(m);
+    int64_t f = (acc[word] >> nw.shift(g)) & nw.mask(g);
+    // a logged carry out of field g took 2^width from it; one out of field
+    // g - 1 added 1 to it
     for (int e = 0; e < nlog; e++) {
-        uint32_t ev = log[e];
-        if ((ev >> 1) != word) continue;
-        if ((ev & 1u) == EV_LOWCARRY)
-            f += half ? -1 : 65536;
-        else if (half)
-            f += 65536;
+        const uint32_t ev = log[e];
+        if ((ev >> 3) != word) continue;
+        const int eg = (int)(ev & 7u);
+        if (eg == g)
+            f += (int64_t)1 << nw.width(g);
+        else if (eg + 1 == g)
+            f -= 1;
     }
     return f;
 }
 
-// C16 counter update: add (1 << 16 * half) to word; fmask selects the field.
-__device__ __forceinline__ void count16(uint32_t *acc, uint32_t word, uint32_t add, uint32_t fmask, int *nlog,
-                                        uint32_t *log, unsigned int *status)
+// Carry-logged narrow counter update: add 1 to field g of word.  A field that
+// was all ones carries into the next (which may carry on in turn; the top
+// field's carry leaves the word): each carry is logged as (word, field), and
+// read_count adds it back.
+__device__ __forceinline__ void count_narrow(uint32_t *acc, uint32_t word, int g, const Narrow &nw, int *nlog,
+                                             uint32_t *log, unsigned int *status)
 {
-    const uint32_t old = atomicAdd(acc + word, add);
-    if ((old & fmask) == fmask) {  // the field was 0xFFFF: it carries
-        const bool low = fmask == 0xFFFFu;
-        const int p0 = atomicAdd(nlog, (low && old == 0xFFFFFFFFu) ? 2 : 1);
-        if (p0 + 1 < LOG_CAP) {
-            if (!low) {
-                log[p0] = (word << 1) | EV_WRAP;
-            } else {
-                log[p0] = (word << 1) | EV_LOWCARRY;
-                if (old == 0xFFFFFFFFu) log[p0 + 1] = (word << 1) | EV_WRAP;
-            }
-        } else {
+    const uint32_t old = atomicAdd(acc + word, 1u << nw.shift(g));
+    for (; g < nw.nf; g++) {
+        const uint32_t mk = nw.mask(g);
+        if (((old >> nw.shift(g)) & mk) != mk) break;
+        const int p0 = atomicAdd(nlog, 1);
+        if (p0 < LOG_CAP)
+            log[p0] = (word << 3) | (uint32_t)g;
+        else
             atomicAdd(status, 1u);
-        }
     }
 }
 
@@ -395,7 +424,7 @@ __device__ __forceinline__ uint32_t load_entry(const void *ent, uint32_t k)
 // windows (rows shorter than the warp count: (window, mask chunk) units split
 // evenly); each lane one neighbour mask per chunk of 32, scanning its bucket
 // four entries at a time (one vector load); the next chunk's bucket bounds
-// are loaded while this chunk's entries are counted.  Counts go to 16-bit
+// are loaded while this chunk's entries are counted.  Counts go to narrow
 // shared fields by plain adds, checked exactly at the end of the item (a
 // carry makes the decoded fields sum to less than the adds made), and the
 // rare item that carried is redone with the carry-logged adds.  Wide counters
@@ -463,9 +492,9 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
     for (int sub_lo = 0; sub_lo < ns; sub_lo += sub) {
         const int sub_n = min(sub, ns - sub_lo);
         const int stride = C16 ? St : sub_n;
-        const int nacc = C16 ? ((a.nlev + 1) / 2) * St : a.nlev * sub_n;
+        const int nacc = C16 ? (a.nw.packed ? St : ((a.nlev + 1) / 2) * St) : a.nlev * sub_n;
         const uint32_t id_lo = max((uint32_t)sub_lo, lo), id_hi = (uint32_t)(sub_lo + sub_n);
-        // 16-bit counters: a first attempt with plain shared adds (no return
+        // narrow counters: a first attempt with plain shared adds (no return
         // value, no per-hit carry test), checked exactly at the end -- the
         // decoded fields sum to the hits counted unless some field carried;
         // only then the item is redone with the carry-logged adds
@@ -482,15 +511,16 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         const bool wide_safe = !C16 && (unsigned long long)nwin * a.wide_bound < (1ull << 32);
         const int nchunk = (n_masks + 31) >> 5;
         // per lane: its mask's bucket (begin, length) and counter slot (C16:
-        // word base of the level pair | the level's half in bit 31; wide: row
-        // base of the level)
+        // word base of the level (0 packed, the level pair's row paired) | the
+        // level's field in bits 29..31; wide: row base of the level)
         auto lane_mask = [&](uint32_t u, int c, uint32_t &b0, uint32_t &n0, uint32_t &sl) {
             b0 = n0 = sl = 0;
             if (c >= n_masks) return;
             const uint32_t mk = masks[c];
             const uint32_t v = u ^ (mk & 0x00FFFFFFu);
             const uint32_t lev = mk >> 24;
-            sl = C16 ? ((lev >> 1) * (uint32_t)St) | ((lev & 1u) << 31) : lev * (uint32_t)stride - (uint32_t)sub_lo;
+            sl = C16 ? (a.nw.packed ? lev << 29 : ((lev >> 1) * (uint32_t)St) | ((lev & 1u) << 29))
+                     : lev * (uint32_t)stride - (uint32_t)sub_lo;
             if (WEIGHTED) {
                 b0 = __ldg(off + v);
                 n0 = __ldg(off + v + 1) - b0;
@@ -510,16 +540,16 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         // slot, and the query window's weight
         uint32_t wq = 1, beg = 0, len = 0, slot = 0;
         // one index entry en of this lane's bucket: counter word base + id
-        // (C16: add `add` to it, the level's 16-bit field; wide: row base).
+        // (C16: add `add` to it, the level's field g; wide: row base).
         // PLAIN (a compile-time flag of the counting loops): C16 plain adds
         // (not the carry-logged retry), wide adds that cannot wrap
-        auto count_hit = [&](auto PLAIN, uint32_t en, uint32_t base, uint32_t add) {
+        auto count_hit = [&](auto PLAIN, uint32_t en, uint32_t base, uint32_t add, int g) {
             constexpr bool plain = decltype(PLAIN)::value;
             const uint32_t id = E16 ? en : (en & 0x00FFFFFFu);
             if (RANGE && (id < id_lo || id >= id_hi)) return;
             if (C16) {
                 if (!plain) {
-                    count16(sm_acc, base + id, add, add * 0xFFFFu, &nlog, sm_log, a.status);
+                    count_narrow(sm_acc, base + id, g, a.nw, &nlog, sm_log, a.status);
                 } else {
                     atomicAdd(sm_acc + base + id, add);
                     if (RANGE) lane_hits++;  // else the chunk's bucket length is counted whole
@@ -547,7 +577,8 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         auto walk = [&](auto PLAIN) {
             constexpr int NB = E16 ? 4 : 2;
             const uint32_t end = beg + len;
-            const uint32_t base = C16 ? slot & 0x7FFFFFFFu : slot, add = C16 ? 1u << ((slot >> 31) * 16u) : 0u;
+            const int g = C16 ? (int)(slot >> 29) : 0;  // the level's field
+            const uint32_t base = C16 ? slot & 0x1FFFFFFFu : slot, add = C16 ? 1u << a.nw.shift(g) : 0u;
             if (!RANGE) lane_hits += len;
             for (uint32_t e = beg & ~3u; __any_sync(GKM_FULL, e < end); e += 4 * NB) {
                 uint32_t en[4 * NB];
@@ -584,7 +615,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                 const uint32_t valid = hi > lo ? ((1u << hi) - 1u) ^ ((1u << lo) - 1u) : 0u;
 #pragma unroll
                 for (int q = 0; q < 4 * NB; q++)
-                    if (valid & (1u << q)) count_hit(PLAIN, en[q], base, add);
+                    if (valid & (1u << q)) count_hit(PLAIN, en[q], base, add, g);
             }
         };
         // the item's windows to the warps, counted in one of two compiled forms
@@ -654,7 +685,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
             unsigned long long fs = 0, hs = lane_hits;
             for (int k = threadIdx.x; k < nacc; k += Q_THREADS) {
                 const uint32_t v = sm_acc[k];
-                fs += (v & 0xFFFFu) + (v >> 16);
+                for (int g = 0; g < a.nw.nf; g++) fs += (v >> a.nw.shift(g)) & a.nw.mask(g);
             }
 #pragma unroll
             for (int o = 16; o; o >>= 1) {
@@ -677,7 +708,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
             for (int s = sub_lo + threadIdx.x; s < sub_lo + sub_n; s += Q_THREADS) {
                 unsigned long long *g = a.gcount + (row * a.S + s0 + s) * a.nlev;
                 for (int m = 0; m < a.nlev; m++) {
-                    const int64_t c = read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo);
+                    const int64_t c = read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo, a.nw);
                     if (c) atomicAdd(g + m, (unsigned long long)c);
                 }
             }
@@ -685,7 +716,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         for (int s = sub_lo + threadIdx.x; s < sub_lo + sub_n; s += Q_THREADS) {
             double k = 0.0;
             for (int m = 0; m < a.nlev; m++)
-                k += a.h[m] * (double)read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo);
+                k += a.h[m] * (double)read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo, a.nw);
             const int64_t sg = s0 + s;
             if (MODE == MODE_SCORE) {
                 const double kn = k * inv_dx * a.inv_ds[sg];
@@ -695,7 +726,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
                 if (a.profile) {
                     uint64_t *pp = a.profile + (row * a.S + sg) * (a.l + 1);
                     for (int m = 0; m <= a.l; m++)
-                        pp[m] = m < a.nlev ? (uint64_t)read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo) : 0;
+                        pp[m] = m < a.nlev ? (uint64_t)read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo, a.nw) : 0;
                 }
             }
         }
@@ -768,10 +799,16 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
     if (spec->weighted && !spec->wd) return gkm_fail(GKM_ERR_INVALID, "weighted spec without weights");
     cudaStream_t st = (cudaStream_t)stream;
     int nlev = spec->dmax + 1;
-    // counter bytes per SV: 16-bit fields (unweighted) or 32-bit (weighted)
+    // counter bytes per SV: narrow fields (unweighted) or 32-bit (weighted)
     int acc_bytes = gkm_smem_limit() - 1024 - (int)query_fixed_smem(n_masks);
-    // 16-bit counters pack two levels of an SV per 32-bit word
-    int per_sv = spec->weighted ? 4 * nlev : 4 * ((nlev + 1) / 2);
+    // narrow counters: every level of an SV in one 32-bit word where the
+    // counts fit fields of these widths (measured per-(row, 36,000-SV tile)
+    // maxima on 256 config-3 queries of 50..2,000 bp, l = 11, d = 3: 14, 59,
+    // 451 and 3,196 per level; a field that overflows is carried exactly by
+    // the per-item check and the carry log), else two 16-bit levels per word
+    static const uint32_t pack4[4] = {4, 7, 9, 12}, pack3[3] = {8, 10, 14};
+    const int packed = !spec->weighted && (nlev == 3 || (nlev == 4 && spec->l <= 11));
+    int per_sv = spec->weighted ? 4 * nlev : packed ? 4 : 4 * ((nlev + 1) / 2);
     int max_tile = (acc_bytes / per_sv) & ~1;
     if (max_tile < 2) return gkm_fail(GKM_ERR_UNSUPPORTED, "%d mismatch levels do not fit shared memory", nlev);
     if (tile_svs <= 0) {
@@ -798,6 +835,8 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
     ix->n_masks = n_masks;
     ix->acc_bytes = acc_bytes;
     ix->wide = spec->weighted ? 1 : 0;
+    ix->packed = packed;
+    for (int m = 0; m < nlev && packed; m++) ix->pack_w[m] = nlev == 4 ? pack4[m] : pack3[m];
     ix->wmax = 1;
     if (spec->weighted) {
         // the largest window weight, from the device table (once per index)
@@ -942,7 +981,7 @@ extern "C" int gkm_index_status(gkm_index_t *ix, uint32_t *counts, int32_t wide,
                                         (cudaStream_t)stream);
         if (e != cudaSuccess) return gkm_cuda_status(e, "index status");
     }
-    // weighted: 32-bit counters, or 64-bit (2); unweighted: 16-bit (0) or 32-bit
+    // weighted: 32-bit counters, or 64-bit (2); unweighted: narrow (0) or 32-bit
     if (wide >= 0) ix->wide = ix->spec.weighted ? (wide == 2 ? 2 : 1) : (wide ? 1 : 0);
     return GKM_OK;
 }
@@ -985,6 +1024,20 @@ static QueryArgs query_args(const gkm_index_t *ix, const uint32_t *bx, const int
     a.wd = ix->spec.wd;
     a.l = ix->spec.l;
     a.wide_bound = (uint64_t)(ix->spec.include_rc ? 2 : 1) * (uint64_t)ix->W * ix->wmax * ix->wmax;
+    a.nw.packed = ix->packed;
+    if (ix->packed) {
+        a.nw.nf = ix->nlev;
+        uint32_t sh = 0;
+        for (int g = 0; g < ix->nlev; g++) {
+            a.nw.fsh |= sh << (5 * g);
+            a.nw.fw |= (ix->pack_w[g] & 31u) << (5 * g);
+            sh += ix->pack_w[g];
+        }
+    } else {
+        a.nw.nf = 2;
+        a.nw.fsh = 16u << 5;
+        a.nw.fw = 16u | (16u << 5);
+    }
     return a;
 }
 

@@ -122,11 +122,11 @@ int gkm_index_info(const gkm_index_t *index, int64_t *entries, int32_t *tiles,
                    int32_t *tile_svs, int64_t *device_bytes);
 /* Copies, in stream order (cudaMemcpyAsync), the index's two event counts
  * into counts[2] (nullable; host or device memory): [0] query blocks whose
- * 16-bit counter carries outgrew their log, [1] 32-bit counters that wrapped.
+ * narrow-counter carries outgrew their log, [1] 32-bit counters that wrapped.
  * The counts only grow: a call whose window (copy before, copy after, on its
  * stream) sees [0] change reruns with 32-bit counters; one that sees [1]
  * change reruns with 64-bit counters (weighted kernels).  wide >= 0 selects,
- * for unweighted kernels, 32-bit counters (1) or 16-bit counters with the
+ * for unweighted kernels, 32-bit counters (1) or narrow counters with the
  * carry log (0); for weighted kernels, 64-bit counters (2) or 32-bit (0, 1).
  * Unweighted 32-bit counters wrap only past 2^32 matching window pairs of one
  * (row, SV) pair; [1] moving there is an error. */
@@ -161,7 +161,7 @@ int gkm_index_score(const gkm_index_t *index, const uint32_t *bx, const int32_t 
  * kept for the life of the device's context: do not call this again on a
  * device after cudaDeviceReset.  All calls share the array, so calls that
  * overlap on the GPU (other streams, other threads) race; serialise them.
- * Exactness, as for gkm_index_score: unweighted indexes count in 16-bit fields
+ * Exactness, as for gkm_index_score: unweighted indexes count in narrow fields
  * with a per-block carry log; a block whose log overflows only raises event
  * count [0] of gkm_index_status, so a caller that needs exact scores reads
  * those counts before and after the call and, if [0] moved, rescores with

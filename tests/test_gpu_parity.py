@@ -463,6 +463,38 @@ def test_weighted_counts_past_32_bits_are_exact():
     np.testing.assert_allclose(_np(m(x)), want, rtol=RTOL, atol=ATOL)
 
 
+def test_packed_counter_carries_are_logged_exactly():
+    """Packed counters (every level of an SV in one 32-bit word, 4 bits for
+    level 0): an 11-mer planted 5 times in 5 SVs and in the query rows makes
+    level-0 counts of 25 (or more), past the field; the item's check sees the
+    carry, the carry-logged retry corrects it within the log (no rerun), and
+    the profiles equal the oracle's."""
+    rng = np.random.default_rng(12)
+    sv = rng.integers(0, 4, (40, 300)).astype(np.uint8)
+    motif = rng.integers(0, 4, 11).astype(np.uint8)
+    for r in range(5):
+        for k in range(5):
+            sv[r, 20 + 55 * k:31 + 55 * k] = motif
+    x = rng.integers(0, 4, (300, 400)).astype(np.uint8)
+    for k in range(5):
+        x[:, 30 + 70 * k:41 + 70 * k] = motif
+    kd = orc.KernelDef.from_params("gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 2.0})
+    want = orc.profiles(x[:3], None, sv, None, kd)
+    assert want[:, :5, 0].min() >= 25
+    m = gk.GkmSVM(sv, rng.normal(size=40), 0.0, "gkmrbf", {"L": 11, "k": 7, "d": 3, "gamma": 2.0}).cuda()
+    m.use_lmer_table = False
+    index = m._sv_index()
+    spec = m._spec()
+    # 300 rows: enough items that no row is split, each row whole in one block
+    fwd, rc, counts = engine.pack(spec, torch.from_numpy(x).cuda(), None)
+    before = index.counters()
+    _, prof = index.pairwise(fwd, counts, raw=False, profile=True, check=False)
+    after = index.counters()
+    torch.cuda.synchronize()
+    assert int(after[0]) == int(before[0])  # every carry fit the log
+    np.testing.assert_array_equal(_np(prof)[:3, :, :4].astype(np.uint64), want[..., :4])
+
+
 @pytest.mark.parametrize("name", ["t2", "t3", "t4", "t5", "t6", "t0"])
 @pytest.mark.parametrize("graphs", [True, False])
 def test_batched_scorer_equals_model(small, name, graphs):
@@ -495,10 +527,11 @@ def test_batched_scorer_config1_table_and_index():
 
 
 def test_bucket_words_of_large_tiles():
-    """48,000 SVs of 500 bp: each of the two SV tiles holds ~23.5M index
-    entries, more than 24 bits of bucket begin, so the bucket words keep 7 bits
-    of length (a bucket of 127 or more entries reads its end from the offsets).
-    Profiles bit-exact to the all-pairs forms, scores equal to the oracle's."""
+    """48,000 SVs of 500 bp: an SV tile holds more than 2^24 index entries
+    (one tile of 47M with packed counters), more bits of bucket begin than 24,
+    so the bucket words keep fewer than 8 bits of length (a bucket that long
+    reads its end from the offsets).  Profiles bit-exact to the all-pairs
+    forms, scores equal to the oracle's."""
     import gkmsvm_lite_b200.synthetic as syn
 
     rng = np.random.default_rng(41)
@@ -513,7 +546,7 @@ def test_bucket_words_of_large_tiles():
     m = gk.GkmSVM(sv, coef, 0.0, "gkmrbf", params).cuda()
     m.use_lmer_table = False
     index = m._sv_index()
-    assert index.tiles == 2 and index.entries / index.tiles > 2**24
+    assert index.entries / index.tiles > 2**24
     spec = m._spec()
     fwd, rc, counts = engine.pack(spec, torch.from_numpy(x).cuda(), xl)
     _, p_index = index.pairwise(fwd, counts, raw=False, profile=True)
