@@ -41,10 +41,10 @@ WORKLOAD = ("config3: 72,000 SVs (200-500 bp, alpha ~ N(0, 0.1^2)), t=3 gkmrbf g
 
 # ncu on a 2,000-query launch of this workload (profiles/index_query_config3_t3_2000q.md):
 # throughput fractions of the units that bind the index query
-NCU_INDEX_QUERY = {"l1tex_data_pipe_frac": 0.862, "lts_throughput_frac": 0.344, "dram_bytes": 1.503e9,
-                   "shared_atomic_wavefronts_frac": 0.375, "global_load_wavefronts_frac": 0.266,
-                   "shared_atomic_bank_conflicts_per_wavefront": 0.60, "issue_active_frac": 0.671,
-                   "warps_active_frac": 0.50}
+NCU_INDEX_QUERY = {"l1tex_data_pipe_frac": 0.762, "lts_throughput_frac": 0.291, "dram_bytes": 3.093e10,
+                   "lts_sector_hit_frac": 0.901, "shared_atomic_wavefronts_frac": 0.319,
+                   "global_load_wavefronts_frac": 0.253, "shared_atomic_bank_conflicts_per_wavefront": 0.57,
+                   "issue_active_frac": 0.589, "warps_active_frac": 0.50}
 
 
 def job_config(queries: int, world: int) -> dict:
@@ -905,9 +905,9 @@ def run_b200(args):
                          "kernel": "index_query (fused SV-tile query + RBF + alpha reduce)",
                          "alg_bytes_per_launch": alg_bytes, "hits": hits, "lookups": lookups,
                          "frac_stored_entry_bytes": stored_bytes / (query_ms / 1e3) / 1e9 / peak,
-                         "binding_unit": "the L1 data pipe (shared adds, bucket and entry gathers) and "
-                                         "instruction issue (the index is L2-resident: HBM is not what "
-                                         "binds it)",
+                         "binding_unit": "the L1 data pipe (shared adds, bucket and entry gathers), "
+                                         "instruction issue and L2 latency (90 % L2 hits; HBM carries "
+                                         "~3 % of its bandwidth: not what binds it)",
                          "ncu_small_case": NCU_INDEX_QUERY,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6.65 TB/s"},
             "stages_ms": {"prep (pack, self-kernels, order)": per_step * 1e3 - query_ms,

@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
     const int St = a.tile_svs;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // persistent: each block takes (tile, row) items off the work queue,
-    // tile-major so that one SV tile's index stays in L2, rows in the order
+    // tile-major so that one SV tile's index is what L2 holds, rows in the order
     // given (longest first)
     for (;;) {
     __syncthreads();
