@@ -96,6 +96,7 @@ class GkmServer:
         self._side: queue.Queue = queue.Queue()
         self._waiting: list[Request] = []
         self._inflight: list = []  # (handle, [requests])
+        self._side_load = 0  # ISM / GkmExplain requests waiting or running
         self._lat: dict = {k: [] for k in KINDS}
         self._seqs = 0
         self._t0 = None
@@ -194,6 +195,8 @@ class GkmServer:
                 r.t_start = time.perf_counter()
             self.admitted += len(batch)
             try:
+                # tells the backend whether side work waits, so it may leave it SMs
+                self.backend.side_busy = self._side_load > 0
                 handle = self.backend.launch_scoring(batch)
             except Exception as e:
                 for r in batch:
@@ -226,6 +229,7 @@ class GkmServer:
                     pending.append(self._side.get_nowait())
             except queue.Empty:
                 pass
+            self._side_load = len(pending)
             if not pending:
                 continue
             # the oldest request's kind (and explain mode), with every waiting
@@ -302,14 +306,17 @@ class GpuBackend:
     direct_rows = 64
 
     def __init__(self, model, slots: int = 2, side_sm_share: float = 1.0, side_graphs: bool = True,
-                 side_pass_positions: int = 128):
+                 side_pass_positions: int = 128, scoring_sm_share: float = 1.0):
         """side_sm_share: the share of the SMs the side worker's persistent
         index queries may take (1: all), so that a scoring pass launched
         meanwhile finds SMs free; side_graphs: ISM / GkmExplain through the
         bucketed graph runners (else direct ism() / gkmexplain() calls);
         side_pass_positions: index-path ISM passes of at most this many
         positions (None: as many as the workspace holds), so that a scoring
-        pass waits for at most one short side kernel."""
+        pass waits for at most one short side kernel; scoring_sm_share: the
+        share of the SMs a scoring pass's persistent index query may take
+        while ISM / GkmExplain work waits (1: all; applies to the passes
+        scored directly, not to the captured graphs of large batches)."""
         import torch
 
         from .batch import BatchedScorer, DirectScorer
@@ -328,6 +335,9 @@ class GpuBackend:
         self.side_stream = torch.cuda.Stream(priority=max(p))
         props = torch.cuda.get_device_properties(model._device)
         self.side_blocks = 0 if side_sm_share >= 1 else max(1, int(props.multi_processor_count * side_sm_share))
+        self.scoring_blocks = (0 if scoring_sm_share >= 1
+                               else max(1, int(props.multi_processor_count * scoring_sm_share)))
+        self.side_busy = False  # set by the server before each scoring launch
         self.side_graphs = side_graphs
         self.side_pass_positions = side_pass_positions
         # ISM / GkmExplain in bucket-shaped CUDA graphs, one runner per kind
@@ -430,6 +440,11 @@ class GpuBackend:
             codes[i, : len(x)] = x
         lens = np.asarray(lens, np.int64)
         stream = self.streams[slot]
+        if self.scoring_blocks:
+            from ._lib import call
+
+            # this (scheduler) thread's index queries: leave SMs to side work that waits
+            call("gkm_set_thread_grid_limit", int(self.scoring_blocks if self.side_busy else 0))
         with torch.cuda.stream(stream):
             xd = torch.from_numpy(codes).pin_memory().to(self.model._device, non_blocking=True)
             ld = torch.from_numpy(lens).pin_memory().to(self.model._device, non_blocking=True)
