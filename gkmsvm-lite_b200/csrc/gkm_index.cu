@@ -342,7 +342,8 @@ struct QueryArgs {
     int skip_empty;       // rows without windows write nothing (their outputs are never read)
     int nsplit;           // items per (row, tile): window ranges of split_w windows
     int split_w;
-    unsigned long long *gcount;  // MODE_COUNT: [B, S, nlev] summed counts
+    unsigned long long *gcount;  // MODE_COUNT: [B, S, nlev] summed counts (gpack: [B, S, (nlev + 1) / 2])
+    int gpack;            // MODE_COUNT: two levels per 64-bit count, 32 bits each (no count reaches 2^32)
     // score
     const double *inv_dx;
     const double *inv_ds;
@@ -706,10 +707,26 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         const int nl = min(nlog, LOG_CAP);
         if (MODE == MODE_COUNT) {
             for (int s = sub_lo + threadIdx.x; s < sub_lo + sub_n; s += Q_THREADS) {
-                unsigned long long *g = a.gcount + (row * a.S + s0 + s) * a.nlev;
-                for (int m = 0; m < a.nlev; m++) {
-                    const int64_t c = read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo, a.nw);
-                    if (c) atomicAdd(g + m, (unsigned long long)c);
+                if (a.gpack) {
+                    // levels 2j and 2j + 1 in one add: half the global atomics
+                    const int gw = (a.nlev + 1) >> 1;
+                    unsigned long long *g = a.gcount + (row * a.S + s0 + s) * gw;
+                    for (int j = 0; j < gw; j++) {
+                        const uint64_t c0 = (uint64_t)read_count<C16, C64>(sm_acc, sm_log, nl, 2 * j, stride,
+                                                                           s - sub_lo, a.nw);
+                        const uint64_t c1 = 2 * j + 1 < a.nlev
+                                                ? (uint64_t)read_count<C16, C64>(sm_acc, sm_log, nl, 2 * j + 1,
+                                                                                 stride, s - sub_lo, a.nw)
+                                                : 0;
+                        const uint64_t v = c0 | (c1 << 32);
+                        if (v) atomicAdd(g + j, (unsigned long long)v);
+                    }
+                } else {
+                    unsigned long long *g = a.gcount + (row * a.S + s0 + s) * a.nlev;
+                    for (int m = 0; m < a.nlev; m++) {
+                        const int64_t c = read_count<C16, C64>(sm_acc, sm_log, nl, m, stride, s - sub_lo, a.nw);
+                        if (c) atomicAdd(g + m, (unsigned long long)c);
+                    }
                 }
             }
         } else
@@ -1113,6 +1130,12 @@ struct CountFinish {
     const unsigned long long *g;
     int64_t B, S;
     int nlev, l, tiles, tile_svs;
+    int gpack;  // two levels per count (see QueryArgs::gpack)
+    __device__ __forceinline__ uint64_t count(int64_t i, int m) const
+    {
+        if (!gpack) return g[i * nlev + m];
+        return (g[i * ((nlev + 1) >> 1) + (m >> 1)] >> (32 * (m & 1))) & 0xFFFFFFFFull;
+    }
     double h[16];
     double *raw;
     uint64_t *profile;
@@ -1126,12 +1149,11 @@ __global__ void count_finish_raw(CountFinish f)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= f.B * f.S) return;
-    const unsigned long long *g = f.g + i * f.nlev;
     double k = 0.0;
-    for (int m = 0; m < f.nlev; m++) k += f.h[m] * (double)g[m];
+    for (int m = 0; m < f.nlev; m++) k += f.h[m] * (double)f.count(i, m);
     if (f.raw) f.raw[i] = k;
     if (f.profile)
-        for (int m = 0; m <= f.l; m++) f.profile[i * (f.l + 1) + m] = m < f.nlev ? (uint64_t)g[m] : 0;
+        for (int m = 0; m <= f.l; m++) f.profile[i * (f.l + 1) + m] = m < f.nlev ? f.count(i, m) : 0;
 }
 
 __global__ void count_finish_score(CountFinish f)
@@ -1143,9 +1165,8 @@ __global__ void count_finish_score(CountFinish f)
     const double inv_dx = f.inv_dx[row];
     double part = 0.0;
     for (int64_t s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
-        const unsigned long long *g = f.g + (row * f.S + s) * f.nlev;
         double k = 0.0;
-        for (int m = 0; m < f.nlev; m++) k += f.h[m] * (double)g[m];
+        for (int m = 0; m < f.nlev; m++) k += f.h[m] * (double)f.count(row * f.S + s, m);
         const double kn = k * inv_dx * f.inv_ds[s];
         part += f.coef[s] * (f.rbf ? exp(f.gamma * (kn - 1.0)) : kn);
     }
@@ -1153,11 +1174,22 @@ __global__ void count_finish_score(CountFinish f)
     if (threadIdx.x == 0) f.partial[row * f.tiles + t] = part;
 }
 
+// split counts hold two levels per 64-bit word when no (row, SV, level) count
+// can reach 2^32: rows of W windows x the SV rows' window slots (both strands)
+// x the largest weight product
+static int split_gpack(const gkm_index_t *ix, int64_t W)
+{
+    const uint64_t bound = (uint64_t)(ix->spec.include_rc ? 2 : 1) * (uint64_t)ix->W * ix->wmax * ix->wmax;
+    return W > 0 && (uint64_t)W < (1ull << 32) / bound;
+}
+
 // the split query into freshly zeroed counts (caller frees *g)
 static int query_split(const gkm_index_t *ix, QueryArgs a, int64_t B, int64_t W, int nsplit,
                        unsigned long long **g, cudaStream_t st)
 {
-    const size_t bytes = sizeof(unsigned long long) * (size_t)(B * ix->S * ix->nlev);
+    a.gpack = split_gpack(ix, W);
+    const int gw = a.gpack ? (ix->nlev + 1) / 2 : ix->nlev;
+    const size_t bytes = sizeof(unsigned long long) * (size_t)(B * ix->S * gw);
     if (cudaMallocAsync((void **)g, bytes, st) != cudaSuccess) return gkm_fail(GKM_ERR_OOM, "split counts");
     cudaError_t e = cudaMemsetAsync(*g, 0, bytes, st);
     if (e != cudaSuccess) return gkm_cuda_status(e, "split counts");
@@ -1168,11 +1200,12 @@ static int query_split(const gkm_index_t *ix, QueryArgs a, int64_t B, int64_t W,
     return query_launch<MODE_COUNT>(ix, a, B, st);
 }
 
-static CountFinish count_finish_args(const gkm_index_t *ix, const unsigned long long *g, int64_t B)
+static CountFinish count_finish_args(const gkm_index_t *ix, const unsigned long long *g, int64_t B, int64_t W)
 {
     CountFinish f = {};
     f.g = g;
     f.B = B;
+    f.gpack = split_gpack(ix, W);
     f.S = ix->S;
     f.nlev = ix->nlev;
     f.l = ix->spec.l;
@@ -1198,7 +1231,7 @@ extern "C" int gkm_index_pairwise(const gkm_index_t *ix, const uint32_t *bx, con
     unsigned long long *g = nullptr;
     int s = query_split(ix, a, B, W, nsplit, &g, st);
     if (s == GKM_OK) {
-        CountFinish f = count_finish_args(ix, g, B);
+        CountFinish f = count_finish_args(ix, g, B, W);
         f.raw = raw;
         f.profile = profile;
         GKM_PREFER_SHARED(count_finish_raw);
@@ -1239,7 +1272,7 @@ extern "C" int gkm_index_score(const gkm_index_t *ix, const uint32_t *bx, const 
         unsigned long long *g = nullptr;
         s = query_split(ix, a, B, W, nsplit, &g, st);
         if (s == GKM_OK) {
-            CountFinish f = count_finish_args(ix, g, B);
+            CountFinish f = count_finish_args(ix, g, B, W);
             f.inv_dx = inv_dx;
             f.inv_ds = inv_ds;
             f.coef = coef;
