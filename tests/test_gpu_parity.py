@@ -397,9 +397,9 @@ def test_encode_10sv_gkmpredict():
 
 
 def test_counter_carries_are_exact():
-    """Low-complexity rows push one (row, SV, level) count past 16 bits: the
-    carry log keeps the counts exact, and a block whose carries outgrow the log
-    is rerun with 32-bit counters."""
+    """Low-complexity rows push one (row, SV, level) count past 16 bits, and
+    far past the narrow fields: counts stay exact whether the carries fit the
+    log or a block outgrows it and the call reruns with 32-bit counters."""
     rng = np.random.default_rng(5)
     sv = np.concatenate([np.zeros((10, 500), np.uint8), rng.integers(0, 4, (30, 500)).astype(np.uint8)])
     coef = rng.normal(size=40)
@@ -412,7 +412,7 @@ def test_counter_carries_are_exact():
     index = m._sv_index()
     spec = m._spec()
     fwd, rc, counts = engine.pack(spec, torch.from_numpy(x).cuda(), None)
-    # one poly-A SV per tile: carries stay within the log
+    # one poly-A SV per tile (exact through the log or the 32-bit rerun)
     ix1 = engine.DeviceIndex(spec, *m._sv_packed(), m._masks(), tile_svs=2)
     raw, prof = ix1.pairwise(fwd, counts, profile=True)
     np.testing.assert_array_equal(_np(prof)[..., :4].astype(np.uint64), want_prof[..., :4])
