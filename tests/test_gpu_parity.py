@@ -141,6 +141,48 @@ def test_ism_index_matches_reference(small, name):
     np.testing.assert_allclose(_np(got), c["ism"], rtol=RTOL, atol=ATOL)
 
 
+@pytest.mark.parametrize("name", ["t3", "t5"])
+def test_index_mutants_with_given_reference_scores(small, name):
+    """gkm_index_mutants through the C ABI with the reference rows' scores
+    passed in (index.score) and with a null ref_score (scored inside the call
+    from ref_raw): the same ISM deltas, equal to gkmsvm-lite's."""
+    from gkmsvm_lite_b200._lib import call, ptr, stream_handle
+    from gkmsvm_lite_b200.ism import ism_workspace
+
+    c = small[name]
+    m = _model(c, use_lmer_table=False)
+    spec, index = m._spec(), m._sv_index()
+    x = torch.from_numpy(np.asarray(c["x"], np.uint8)).cuda()
+    xl = None if c["x_lengths"] is None else torch.as_tensor(np.asarray(c["x_lengths"], np.int64)).cuda()
+    fwd, rc, counts = engine.pack(spec, x, xl)
+    B, W = fwd.shape
+    L = x.shape[1]
+    from gkmsvm_lite_b200.kernels import RbfKernel
+
+    kernel = m.kernel
+    rbf = isinstance(kernel, RbfKernel)
+    gamma = kernel.gamma if rbf else 0.0
+    diag = engine.self_kernel(spec, fwd, rc, counts)
+    mut = engine.mutant_diag(spec, fwd, counts, L, diag)
+    inv_dx = 1.0 / torch.sqrt(torch.clamp(diag, min=1e-20))
+    inv_dmut = 1.0 / torch.sqrt(torch.clamp(mut, min=1e-20))
+    ref_raw, _ = index.pairwise(fwd, counts)
+    ref_score = index.score(fwd, counts, inv_dx, m._inv_ds(), m._sv_coef(), gamma, rbf, 0.0)
+    work = ism_workspace(m, B, L, fwd.device)
+    outs = []
+    for given in (ref_score, None):
+        out = torch.empty((B, 4, L), dtype=torch.float64, device=fwd.device)
+        call("gkm_index_mutants", index.handle, ptr(fwd), ptr(counts), B, W, L, ptr(ref_raw), ptr(given),
+             ptr(inv_dx), ptr(inv_dmut), ptr(m._inv_ds()), ptr(m._sv_coef()), float(gamma), int(rbf),
+             ptr(out), ptr(work), int(work.numel()), stream_handle())
+        torch.cuda.synchronize()
+        outs.append(_np(out))
+    want = np.asarray(c["ism"], np.float64)
+    for got in outs:
+        ok = np.isfinite(want)
+        np.testing.assert_allclose(got[ok], want[ok], rtol=RTOL, atol=ATOL)
+
+
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("mode,key", [("hypothetical", "explain_hyp"), ("importance", "explain_imp"),
                                       ("perturbation", "explain_pert")])
