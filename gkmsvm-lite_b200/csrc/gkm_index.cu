@@ -821,10 +821,13 @@ extern "C" int gkm_index_create(const gkm_spec *spec, const uint32_t *fwd, const
     // narrow counters: every level of an SV in one 32-bit word where the
     // counts fit fields of these widths (measured per-(row, 36,000-SV tile)
     // maxima on 256 config-3 queries of 50..2,000 bp, l = 11, d = 3: 14, 59,
-    // 451 and 3,196 per level; a field that overflows is carried exactly by
-    // the per-item check and the carry log), else two 16-bit levels per word
+    // 451 and 3,196 per level; random matches grow 4x for each l below, so
+    // d = 3 packs at l = 11..12 and d = 2 (8 / 10 / 14 bits) at l >= 8; a field
+    // that overflows is carried exactly by the per-item check and the carry
+    // log), else two 16-bit levels per word
     static const uint32_t pack4[4] = {4, 7, 9, 12}, pack3[3] = {8, 10, 14};
-    const int packed = !spec->weighted && (nlev == 3 || (nlev == 4 && spec->l <= 11));
+    const int packed = !spec->weighted && ((nlev == 4 && spec->l >= 11 && spec->l <= 12) ||
+                                           (nlev == 3 && spec->l >= 8));
     int per_sv = spec->weighted ? 4 * nlev : packed ? 4 : 4 * ((nlev + 1) / 2);
     int max_tile = (acc_bytes / per_sv) & ~1;
     if (max_tile < 2) return gkm_fail(GKM_ERR_UNSUPPORTED, "%d mismatch levels do not fit shared memory", nlev);
