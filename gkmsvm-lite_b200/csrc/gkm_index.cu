@@ -573,10 +573,13 @@ __global__ void __launch_bounds__(Q_THREADS, 1) index_query(QueryArgs a)
         // before any is counted; the warp runs as many iterations as its
         // longest bucket needs.  Measured: 2-byte entries (8-byte blocks) 2
         // blocks 417 ms, 3: 405, 4: 401 on 5,000 config-3 queries, one block
-        // 500; 4-byte entries (16-byte blocks) 1 block 1,841 ms, 2: 1,591, 4:
-        // 1,753 on 10,000 config-3 queries of the weighted t=5 kernel
+        // 500; with packed counters (larger buckets) 4: 341.6 ms, 5: 340.5, 6:
+        // 338.1, six spilling registers where the SV range is tested (RANGE);
+        // 4-byte entries (16-byte blocks) 1 block 1,841 ms, 2: 1,591, 4: 1,753
+        // on 10,000 config-3 queries of the weighted t=5 kernel (3: 2 % faster
+        // there, 5 % slower on the config-2 Gram)
         auto walk = [&](auto PLAIN) {
-            constexpr int NB = E16 ? 4 : 2;
+            constexpr int NB = E16 ? (RANGE ? 4 : 6) : 2;
             const uint32_t end = beg + len;
             const int g = C16 ? (int)(slot >> 29) : 0;  // the level's field
             const uint32_t base = C16 ? slot & 0x1FFFFFFFu : slot, add = C16 ? 1u << a.nw.shift(g) : 0u;
