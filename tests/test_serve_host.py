@@ -176,3 +176,32 @@ def test_side_worker_yields_to_scoring_passes():
         srv.submit("ism", np.ones((1, 5))).result(10)
         assert time.perf_counter() - t0 < 2.0
     assert be.side_started_with_inflight == [1]
+
+
+def test_backend_told_when_side_work_waits():
+    """Before each scoring launch the server sets backend.side_busy: True while
+    ISM / GkmExplain requests wait or run, False when none do."""
+
+    class Recording(FakeBackend):
+        def __init__(self):
+            super().__init__(delay=0.01)
+            self.seen = []
+
+        def launch_scoring(self, batch):
+            self.seen.append(getattr(self, "side_busy", None))
+            return super().launch_scoring(batch)
+
+        def run_side(self, r):
+            time.sleep(0.3)
+            return np.asarray(r.x) * 2.0
+
+    be = Recording()
+    with GkmServer(be, memory_reserve=0) as srv:
+        srv.submit("predict", np.ones((1, 5))).result(10)
+        side = srv.submit("ism", np.ones((1, 5)))
+        time.sleep(0.05)  # the side call is running
+        srv.submit("predict", np.ones((1, 5))).result(10)
+        side.result(10)
+        time.sleep(0.05)
+        srv.submit("predict", np.ones((1, 5))).result(10)
+    assert be.seen == [False, True, False]
